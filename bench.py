@@ -1,0 +1,382 @@
+"""Benchmark of the B200 state-vector backend (one JSON line on rank 0).
+
+Workload (the headline configuration): a seeded random brick circuit on
+30 qubits, complex<double> (16 GiB state), depth 200 -- per layer one gate
+from {Hadamard, RotationX, RotationY, RotationZ} on every qubit, then CNOT
+or CZ on alternating neighbour pairs: 8,900 gates.  One step = reset to
+|0...0> + the whole circuit through the fused sweep, state resident in HBM.
+The state (16 GiB) is far larger than L2 (126 MB), so no flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank simulates its own
+circuit (replicas, weak scaling; the path has no exchange step); time is the
+max over ranks.  ``--impl reference`` times QCLAB++'s own CPU simulate
+(compiled from its sources into oracle/_ref) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "gates/s & HBM GB/s vs 8TB/s at 30q; adjoint grads/s vs param-shift @1e-9"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--qubits", type=int, default=30)
+    p.add_argument("--depth", type=int, default=200)
+    p.add_argument("--seed", type=int, default=2024)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--unfused-gates", type=int, default=45)
+    return p.parse_args()
+
+
+def peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_per_launch(n, elem_bytes):
+    """DRAM bytes per fused-stage launch from the committed ncu summary,
+    scaled to this state size (traffic grows with the amplitudes moved)."""
+    f = ROOT / "profiles" / "k_stage_traffic.json"
+    if not f.exists():
+        return None
+    d = json.loads(f.read_text())
+    per_amp = d.get("dram_bytes_per_amplitude", {}).get(str(elem_bytes))
+    if per_amp is None:
+        return None
+    return float(per_amp) * (1 << n)
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(f"/tmp/qsv_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return None
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        smax = max((num(r[2]) for r in rows if num(r[2]) is not None), default=None)
+        power = [num(r[3]) for r in rows if num(r[3]) is not None]
+        loaded = [s for s, p in zip(sm, power) if p is not None and p > 250] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_reference_sample(n, recs, budget_s=15.0):
+    """QCLAB++'s CPU simulate (oracle/_ref, all host threads) on a bounded
+    slice of the circuit; returns (gates/s, threads, kind, sample text)."""
+    import oracle
+    dtype = np.complex128
+    kind = "reference" if oracle.ref_available() else "port"
+    if kind == "port":
+        # the C oracle: single-threaded restatement; time a slice at 24 qubits
+        n_s = min(n, 24)
+        from qclab_b200 import workloads as W
+        sub = [r for r in recs if max(r["qubit0"], r["qubit1"]) < n_s][:200]
+        sub = np.array(sub, dtype=recs.dtype)
+        x = np.zeros(1 << n_s, dtype=dtype)
+        x[0] = 1
+        t0 = time.perf_counter()
+        oracle.apply(x, sub)
+        dt = time.perf_counter() - t0
+        return len(sub) / dt * (1 << n_s) / (1 << n), 1, kind, (
+            f"C oracle, 1 thread, first {len(sub)} gates at {n_s} qubits, scaled by 2^{n - n_s}")
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 1 << 40
+    n_s = n
+    while n_s > 20 and (1 << n_s) * 16 * 2.5 > avail:
+        n_s -= 1
+    # one gate first to size the sample
+    one = oracle.RefCircuit(n_s, dtype, recs[:1])
+    one.state[:] = 0
+    one.state[0] = 1
+    t0 = time.perf_counter()
+    one.apply()
+    per_gate = time.perf_counter() - t0
+    one.close()
+    g = int(max(5, min(len(recs), budget_s / max(per_gate, 1e-6))))
+    sub = recs[:g]
+    rc = oracle.RefCircuit(n_s, dtype, sub)
+    rc.state[:] = 0
+    rc.state[0] = 1
+    t0 = time.perf_counter()
+    rc.apply()
+    dt = time.perf_counter() - t0
+    threads = oracle.ref_threads()
+    rc.close()
+    scale = (1 << n_s) / (1 << n)
+    txt = (f"QCLAB++ QCircuit::simulate (g++ -O3 -fopenmp), {threads} threads, first {g} gates "
+           f"of the circuit at {n_s} qubits" + (f", scaled by 2^{n - n_s}" if n_s != n else ""))
+    return g / dt * scale, threads, kind, txt
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    from qclab_b200 import workloads as W
+    recs = W.brick(args.qubits, args.depth, seed=args.seed).gate_records(np.complex128)
+    vals = []
+    threads, kind, txt = 0, "reference", ""
+    for i in range(args.warmup + args.steps):
+        v, threads, kind, txt = cpu_reference_sample(args.qubits, recs, budget_s=8.0)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "gates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c128", "data": "synthetic: seeded random brick circuit, |0...0> input",
+        "config": workload_config(args, len(recs), world),
+        "cpu_baseline": {"value": value, "unit": "gates/s", "cores": threads, "kind": kind,
+                         "sample": txt},
+        "e2e": {"value": value, "unit": "gates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args, ngates, world):
+    return {"workload": f"brick{args.qubits}_depth{args.depth}_c128", "qubits": args.qubits,
+            "depth": args.depth, "gates": ngates, "seed": args.seed,
+            "parallelism": f"replicas{world}" if world > 1 else "single",
+            "path": "fused sweep (qsv_apply_fused)",
+            "l2": "no flush: the 16 GiB state is larger than L2 (126 MB)"}
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    from qclab_b200 import StateVector, launch_count
+    from qclab_b200 import _lib as L
+    from qclab_b200 import workloads as W
+
+    n = args.qubits
+    circ = W.brick(n, args.depth, seed=args.seed + rank)
+    recs = circ.gate_records(np.complex128)
+    ngates = len(recs)
+    stream = torch.cuda.current_stream()
+    sv = StateVector(n, np.complex128)
+    sv.set_stream(stream.cuda_stream)
+    opts = L.FuseOpts(profile=1)
+    lib = L.load()
+
+    def step():
+        sv.set_basis(0)
+        sv.apply(recs, "N", 0, fused=True, opts=opts)
+
+    def stage_times():
+        cnt = C.c_int(0)
+        lib.qsv_last_stage_times(None, 0, C.byref(cnt))
+        buf = (C.c_float * cnt.value)()
+        lib.qsv_last_stage_times(buf, cnt.value, C.byref(cnt))
+        return list(buf)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    launches0 = launch_count()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0.record(stream)
+    stage_ms = []
+    for _ in range(args.steps):
+        step()
+        stage_ms.extend(stage_times())
+    t1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = t0.elapsed_time(t1)
+    launches = launch_count() - launches0
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * ngates * args.steps / (ms / 1e3)
+
+    # roofline of the dominant kernel (the fused stage sweep)
+    n_stages = len(stage_ms) // max(args.steps, 1)
+    state_bytes = (1 << n) * 16
+    alg_bytes = 2 * state_bytes
+    avg_stage_ms = statistics.mean(stage_ms) if stage_ms else float("nan")
+    achieved = alg_bytes / (avg_stage_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = traffic_per_launch(n, 16)
+    roofline = {"bound": "hbm", "kernel": "k_stage<double2> (fused stage sweep)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": f"{peak_kind} hbm_gbs", "traffic": traffic,
+                "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_stage_ms,
+                "launches_per_step": n_stages}
+
+    # unfused reference-exact path on the first layer (side measurement)
+    unf = None
+    if args.unfused_gates > 0:
+        sub = recs[:args.unfused_gates]
+        sv.set_basis(0)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sv.apply(sub, "N", 0, fused=False)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ums = a.elapsed_time(b)
+        unf_bytes = 0
+        for r in sub:
+            k = int(r["kind"])
+            unf_bytes += state_bytes * (2 if k in (L.HADAMARD, L.ROTATION_X, L.ROTATION_Y, L.ROTATION_Z)
+                                        else 1 if k == L.CX else 0.5)
+        unf = {"gates": len(sub), "gates_per_s": len(sub) / (ums / 1e3),
+               "hbm_gbs": unf_bytes / (ums / 1e3) / 1e9, "path": "qsv_apply (bit-exact)"}
+
+    # end to end through the C ABI with host buffers (copies inside the timed region)
+    e2e = None
+    if not args.no_e2e:
+        try:
+            host = torch.zeros(1 << n, dtype=torch.complex128, pin_memory=True)
+            host[0] = 1
+            hp = host.data_ptr()
+            e_steps = max(1, min(args.steps, 2))
+            torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(e_steps):
+                sv.upload_ptr(hp, state_bytes)
+                sv.apply(recs, "N", 0, fused=True)
+                sv.download_ptr(hp, state_bytes)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ems = a.elapsed_time(b)
+            if world > 1:
+                t = torch.tensor([ems], dtype=torch.float64, device="cuda")
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                ems = float(t.item())
+            e2e = {"value": world * ngates * e_steps / (ems / 1e3), "unit": "gates/s",
+                   "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                   "steps": e_steps, "ms_per_step": ems / e_steps,
+                   "api": "qsv_upload + qsv_apply_fused + qsv_download (pinned host buffer)"}
+            del host
+        except Exception as ex:  # pinned allocation can fail on small hosts
+            e2e = {"value": None, "unit": "gates/s", "h2d_bytes_per_step": state_bytes,
+                   "d2h_bytes_per_step": state_bytes, "error": str(ex)[:200]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, threads, kind, txt = cpu_reference_sample(n, recs)
+        cpu = {"value": v, "unit": "gates/s", "cores": threads, "kind": kind, "sample": txt}
+
+    sv.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "gates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic: seeded random brick circuit, |0...0> input",
+            "config": workload_config(args, ngates, world),
+            "hbm_gbs_algorithmic": n_stages * alg_bytes / (ms_per_step / 1e3) / 1e9,
+            "hbm_gbs_effective_unfused_equivalent": None,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": launches, "unfused_first_layer": unf,
+        }
+        eff = 0
+        for r in recs:
+            k = int(r["kind"])
+            eff += state_bytes * (2 if k in (L.HADAMARD, L.ROTATION_X, L.ROTATION_Y, L.ROTATION_Z)
+                                  else 1 if k == L.CX else 0.5)
+        line["hbm_gbs_effective_unfused_equivalent"] = eff / (ms_per_step / 1e3) / 1e9
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,188 @@
+/*
+ * qclab_b200.h -- C ABI of the B200 state-vector backend for QCLAB++.
+ *
+ * Every entry point is plain C: integers, doubles, raw pointers and sizes.
+ * Every entry point returns a qsv_status (0 = success) and never aborts;
+ * qsv_last_error() returns a message for the last failure on the calling
+ * thread.  All device work is issued on the state's CUDA stream (the legacy
+ * default stream unless qsv_set_stream was called); calls that return host
+ * values (downloads, reductions) synchronise that stream.
+ *
+ * Conventions follow QCLAB++ exactly:
+ *   - qubit q of an n-qubit register is bit (n-1-q) of the amplitude index
+ *     (qubit 0 is the most significant bit)      [src/qgates/apply.hpp:227-238]
+ *   - an op is 'N' (NoTrans), 'T' (Trans) or 'C' (ConjTrans) and is applied
+ *     to every gate; for 'T'/'C' the gate list runs in reverse order
+ *                                               [include/qclab/QCircuit.hpp:130-143]
+ *   - rotations carry cos/sin of theta/2 (QRotation), Phase and CPhase carry
+ *     cos/sin of theta (QAngle)     [include/qclab/QRotation.hpp:44-66,
+ *                                    include/qclab/QAngle.hpp:30-48]
+ *   - dense matrices are column-major, complex entries stored as (re, im)
+ *                                    [include/qclab/dense/SquareMatrix.hpp:57-78]
+ */
+#ifndef QCLAB_B200_H
+#define QCLAB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QSV_ABI_VERSION 1
+
+typedef enum qsv_status {
+  QSV_SUCCESS             = 0,
+  QSV_ERROR_INVALID_VALUE = 1,  /* null pointer, unknown enum, bad op char   */
+  QSV_ERROR_QUBIT         = 2,  /* qubit outside [0,nbQubits) or repeated    */
+  QSV_ERROR_SIZE          = 3,  /* byte count or problem size out of range   */
+  QSV_ERROR_CUDA          = 4,  /* CUDA runtime failure (see qsv_last_error) */
+  QSV_ERROR_OUT_OF_MEMORY = 5,  /* device allocation failed                  */
+  QSV_ERROR_DTYPE         = 6,  /* gate not defined for a real element type  */
+  QSV_ERROR_TIMEOUT       = 7,  /* a bounded device-side wait expired        */
+  QSV_ERROR_NOT_SUPPORTED = 8
+} qsv_status;
+
+/* Element type of a state vector (the QCLAB++ template parameter T). */
+typedef enum qsv_dtype {
+  QSV_C64  = 0,   /* std::complex<float>  */
+  QSV_C128 = 1,   /* std::complex<double> */
+  QSV_F32  = 2,   /* float                */
+  QSV_F64  = 3    /* double               */
+} qsv_dtype;
+
+/* Gate kinds: one per QCLAB++ gate class on the state-vector path, plus the
+ * generic matrix gates (U2/U3/MatrixGate) that QCLAB++ lacks.               */
+typedef enum qsv_gate_kind {
+  QSV_IDENTITY      = 0,   /* qgates/Identity                                 */
+  QSV_HADAMARD      = 1,   /* qgates/Hadamard                                 */
+  QSV_PAULI_X       = 2,   /* qgates/PauliX                                   */
+  QSV_PAULI_Y       = 3,   /* qgates/PauliY                                   */
+  QSV_PAULI_Z       = 4,   /* qgates/PauliZ                                   */
+  QSV_ROTATION_X    = 5,   /* qgates/RotationX   (cos,sin of theta/2)         */
+  QSV_ROTATION_Y    = 6,   /* qgates/RotationY   (cos,sin of theta/2)         */
+  QSV_ROTATION_Z    = 7,   /* qgates/RotationZ   (cos,sin of theta/2)         */
+  QSV_PHASE         = 8,   /* qgates/Phase       (cos,sin of theta)           */
+  QSV_PHASE45       = 9,   /* qgates/Phase45 (T gate)                         */
+  QSV_PHASE90       = 10,  /* qgates/Phase90 (S gate)                         */
+  QSV_MATRIX1       = 11,  /* QGate1 / PointerGate1 / U2 / U3: matrix[0..7]   */
+  QSV_CX            = 12,  /* qgates/CX (= CNOT)                              */
+  QSV_CY            = 13,  /* qgates/CY                                       */
+  QSV_CZ            = 14,  /* qgates/CZ                                       */
+  QSV_CPHASE        = 15,  /* qgates/CPhase      (cos,sin of theta)           */
+  QSV_CROTATION_X   = 16,  /* qgates/CRotationX  (cos,sin of theta/2)         */
+  QSV_CROTATION_Y   = 17,  /* qgates/CRotationY  (cos,sin of theta/2)         */
+  QSV_CROTATION_Z   = 18,  /* qgates/CRotationZ  (cos,sin of theta/2)         */
+  QSV_CONTROLLED1   = 19,  /* QControlledGate2 with any 2x2 target matrix     */
+  QSV_SWAP          = 20,  /* qgates/SWAP                                     */
+  QSV_ISWAP         = 21,  /* qgates/iSWAP                                    */
+  QSV_ROTATION_XX   = 22,  /* qgates/RotationXX  (cos,sin of theta/2)         */
+  QSV_ROTATION_YY   = 23,  /* qgates/RotationYY  (cos,sin of theta/2)         */
+  QSV_ROTATION_ZZ   = 24,  /* qgates/RotationZZ  (cos,sin of theta/2)         */
+  QSV_MATRIX2       = 25,  /* QGate2 / PointerGate2 / MatrixGate2: 4x4        */
+  QSV_NUM_GATE_KINDS = 26
+} qsv_gate_kind;
+
+/*
+ * One gate record (the flat form of a qclab::QObject<T> gate).
+ *   1-qubit kinds     : qubit0 = the qubit.
+ *   controlled kinds  : qubit0 = control, qubit1 = target, control_state 0/1.
+ *   SWAP/iSWAP/RXX/RYY/RZZ : qubit0, qubit1 in any order (sorted as QCLAB++
+ *                       does, include/qclab/qgates/QRotationGate2.hpp:142-147).
+ *   MATRIX2           : 4x4 in the basis |qubit0 qubit1>, qubit0 the leading
+ *                       tensor factor (either order of qubit0/qubit1 allowed).
+ *   param             : index of the trainable angle this gate depends on
+ *                       (adjoint gradients), or -1.
+ */
+typedef struct qsv_gate {
+  int32_t kind;
+  int32_t qubit0;
+  int32_t qubit1;
+  int32_t control_state;
+  double  cos;
+  double  sin;
+  double  matrix[32];
+  int32_t param;
+  int32_t reserved;
+} qsv_gate;
+
+typedef struct qsv_state_s* qsv_state;
+
+/* ---- library ------------------------------------------------------------ */
+int         qsv_abi_version(void);
+const char* qsv_last_error(void);
+const char* qsv_status_string(qsv_status status);
+/* number of kernel launches this library has issued on the calling thread */
+uint64_t    qsv_launch_count(void);
+
+/* ---- state vectors ------------------------------------------------------ */
+/* Allocates a 2^nbQubits state on the current device, set to |0...0>.
+ * Replaces std::vector<T>(N) + psi[0]=1 of test/timings/run.hpp:50-52.     */
+qsv_status qsv_create(int nbQubits, qsv_dtype dtype, qsv_state* out);
+/* Non-owning view of caller-owned device memory (QCLAB++'s device T*,
+ * QCircuit::simulate_device, include/qclab/QCircuit.hpp:170-172).          */
+qsv_status qsv_wrap(int nbQubits, qsv_dtype dtype, void* device_ptr,
+                    qsv_state* out);
+qsv_status qsv_destroy(qsv_state state);
+qsv_status qsv_set_stream(qsv_state state, void* cuda_stream);
+qsv_status qsv_info(qsv_state state, int* nbQubits, qsv_dtype* dtype,
+                    void** device_ptr);
+qsv_status qsv_upload(qsv_state state, const void* host, size_t bytes);
+qsv_status qsv_download(qsv_state state, void* host, size_t bytes);
+qsv_status qsv_copy(qsv_state dst, qsv_state src);
+/* |index> (a computational basis state, big-endian qubit order). */
+qsv_status qsv_set_basis(qsv_state state, uint64_t index);
+qsv_status qsv_synchronize(qsv_state state);
+
+/* ---- gate application --------------------------------------------------- */
+/* Reference-exact path: one kernel per gate, with the operation order of the
+ * reference lambdas and no FMA contraction, so results are bitwise equal to
+ * QCLAB++'s CPU apply.  Replaces QObject<T>::apply(Op, nbQubits, vector,
+ * offset) (include/qclab/QObject.hpp:52-53) and the QCircuit gate loop
+ * (include/qclab/QCircuit.hpp:130-143).                                     */
+qsv_status qsv_apply(qsv_state state, const qsv_gate* gates, size_t nGates,
+                     char op, int offset);
+
+/* Options of the fused sweep. Zero-initialised fields pick tuned defaults. */
+typedef struct qsv_fuse_opts {
+  int tile_bits;     /* m: amplitudes per shared-memory tile = 2^m           */
+  int low_bits;      /* L: contiguous low bits always in the tile            */
+  int reg_bits;      /* k: qubits per register block inside a tile           */
+  int max_stage_gates;
+  int profile;       /* 1: time every stage with CUDA events (see below)   */
+  int reserved[3];
+} qsv_fuse_opts;
+
+/* Fused path: the gate list is planned into stages; each stage streams the
+ * state through shared memory once and applies all of its gates there.
+ * Within 1e-12 (complex<double>) of qsv_apply, not bitwise.               */
+qsv_status qsv_apply_fused(qsv_state state, const qsv_gate* gates,
+                           size_t nGates, char op, int offset,
+                           const qsv_fuse_opts* opts);
+
+/* Per-stage kernel durations (ms, CUDA events on the state's stream) of the
+ * last qsv_apply_fused call on this thread that ran with opts->profile = 1.
+ * Synchronises nothing; the profiled call already waited for its events. */
+qsv_status qsv_last_stage_times(float* ms, int capacity, int* count);
+
+/* Plan statistics for a gate list (no device work): number of stages and
+ * of gates per stage.  stage_gates may be NULL.                            */
+qsv_status qsv_plan_stats(int nbQubits, qsv_dtype dtype, const qsv_gate* gates,
+                          size_t nGates, char op, int offset,
+                          const qsv_fuse_opts* opts, int* nStages,
+                          int* stage_gates, int capacity);
+
+/* Host-buffer convenience, the drop-in for QCircuit<T>::simulate(vector)
+ * (include/qclab/QCircuit.hpp:164-166): copies `host` (2^nbQubits elements
+ * of dtype) to the device, applies the gate list with `op`, copies back.
+ * fused != 0 selects qsv_apply_fused.                                      */
+qsv_status qsv_apply_host(int nbQubits, qsv_dtype dtype, void* host,
+                          const qsv_gate* gates, size_t nGates, char op,
+                          int offset, int fused);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QCLAB_B200_H */

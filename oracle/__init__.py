@@ -1,0 +1,177 @@
+"""CPU oracle for the QCLAB++ state-vector path -- TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this package, and only as the checker.  The product
+(``qclab_b200``) never imports it.
+
+* ``apply``: the plain-C restatement in ``qsv_oracle.c`` (built to
+  ``liboracle.so`` with gcc, no FMA contraction).
+* ``Ref``: QCLAB++ itself, compiled from its own sources into
+  ``_ref/libqclab_ref.so`` (``oracle/Makefile``; only where the reference
+  tree exists -- the library then travels with the repository).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libqclab_ref.so"
+REF_TESTS = HERE / "_ref" / "ref_tests"
+
+DTYPE_CODE = {np.dtype(np.complex64): 0, np.dtype(np.complex128): 1,
+              np.dtype(np.float32): 2, np.dtype(np.float64): 3}
+
+_lock = threading.Lock()
+_lib = None
+_ref = None
+
+
+def build() -> None:
+    """Builds liboracle.so (always) and _ref/ (when the reference tree exists)."""
+    env = dict(os.environ)
+    env.pop("CC", None)
+    env.pop("CXX", None)
+    r = subprocess.run(["make", "-C", str(HERE), "-j8", "all"], capture_output=True, text=True,
+                       env=env)
+    if r.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{r.stdout[-4000:]}\n{r.stderr[-4000:]}")
+
+
+def _build_oracle_only() -> None:
+    env = dict(os.environ)
+    env.pop("CC", None)
+    env.pop("CXX", None)
+    r = subprocess.run(["make", "-C", str(HERE), "liboracle.so"], capture_output=True, text=True,
+                       env=env)
+    if r.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{r.stdout[-4000:]}\n{r.stderr[-4000:]}")
+
+
+def load():
+    global _lib
+    with _lock:
+        if _lib is None:
+            src = HERE / "qsv_oracle.c"
+            if not LIB.exists() or LIB.stat().st_mtime < max(
+                    src.stat().st_mtime, (HERE / "oracle_impl.h").stat().st_mtime):
+                _build_oracle_only()
+            lib = C.CDLL(str(LIB))
+            lib.oracle_apply.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_size_t,
+                                         C.c_char, C.c_int]
+            lib.oracle_apply.restype = C.c_int
+            lib.oracle_cosf.argtypes = [C.c_float]
+            lib.oracle_cosf.restype = C.c_float
+            lib.oracle_sinf.argtypes = [C.c_float]
+            lib.oracle_sinf.restype = C.c_float
+            _lib = lib
+        return _lib
+
+
+def _records(recs):
+    from qclab_b200 import _lib as L
+    if isinstance(recs, np.ndarray) and recs.dtype == L.GATE_DTYPE:
+        return np.ascontiguousarray(recs)
+    return np.array(list(recs), dtype=L.GATE_DTYPE)
+
+
+def apply(state: np.ndarray, recs, op: str = "N", offset: int = 0) -> np.ndarray:
+    """Applies gate records to ``state`` (host, in place) with the C oracle."""
+    lib = load()
+    r = _records(recs)
+    n = int(state.size).bit_length() - 1
+    if state.size != 1 << n or not state.flags.c_contiguous:
+        raise ValueError("state must be a contiguous power-of-two vector")
+    st = lib.oracle_apply(n, DTYPE_CODE[state.dtype], state.ctypes.data,
+                          r.ctypes.data if len(r) else None, len(r), op.encode(), int(offset))
+    if st != 0:
+        raise RuntimeError(f"oracle_apply failed with status {st}")
+    return state
+
+
+def ref_available() -> bool:
+    return REF_LIB.exists()
+
+
+def _load_ref():
+    global _ref
+    with _lock:
+        if _ref is None:
+            lib = C.CDLL(str(REF_LIB))
+            lib.ref_circuit_create.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_size_t,
+                                               C.POINTER(C.c_int)]
+            lib.ref_circuit_create.restype = C.c_void_p
+            lib.ref_circuit_destroy.argtypes = [C.c_void_p]
+            lib.ref_vec_create.argtypes = [C.c_int, C.c_uint64]
+            lib.ref_vec_create.restype = C.c_void_p
+            lib.ref_vec_data.argtypes = [C.c_void_p]
+            lib.ref_vec_data.restype = C.c_void_p
+            lib.ref_vec_destroy.argtypes = [C.c_void_p]
+            lib.ref_circuit_apply.argtypes = [C.c_void_p, C.c_void_p, C.c_char, C.c_int]
+            lib.ref_circuit_apply.restype = C.c_int
+            lib.ref_num_threads.restype = C.c_int
+            lib.ref_set_num_threads.argtypes = [C.c_int]
+            _ref = lib
+        return _ref
+
+
+class RefCircuit:
+    """A QCLAB++ ``QCircuit<T>`` built from records, with a driver-owned
+    ``std::vector<T>`` state (exposed as a numpy view)."""
+
+    def __init__(self, n: int, dtype, recs):
+        self.lib = _load_ref()
+        self.n = n
+        self.dtype = np.dtype(dtype)
+        r = _records(recs)
+        st = C.c_int(0)
+        self.c = self.lib.ref_circuit_create(n, DTYPE_CODE[self.dtype],
+                                             r.ctypes.data if len(r) else None, len(r),
+                                             C.byref(st))
+        if not self.c:
+            raise RuntimeError(f"reference circuit construction failed ({st.value})")
+        self.v = self.lib.ref_vec_create(DTYPE_CODE[self.dtype], 1 << n)
+        ptr = self.lib.ref_vec_data(self.v)
+        buf = (C.c_char * ((1 << n) * self.dtype.itemsize)).from_address(ptr)
+        self.state = np.frombuffer(buf, dtype=self.dtype)
+
+    def apply(self, op: str = "N", offset: int = 0) -> None:
+        st = self.lib.ref_circuit_apply(self.c, self.v, op.encode(), int(offset))
+        if st != 0:
+            raise RuntimeError(f"reference apply failed ({st})")
+
+    def close(self) -> None:
+        if self.c:
+            self.lib.ref_circuit_destroy(self.c)
+            self.c = None
+        if self.v:
+            self.state = None
+            self.lib.ref_vec_destroy(self.v)
+            self.v = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ref_apply(state: np.ndarray, recs, op: str = "N", offset: int = 0) -> np.ndarray:
+    """Runs the reference's QCircuit::apply on a copy of ``state``."""
+    n = int(state.size).bit_length() - 1
+    rc = RefCircuit(n, state.dtype, recs)
+    rc.state[:] = state
+    rc.apply(op, offset)
+    out = rc.state.copy()
+    rc.close()
+    return out
+
+
+def ref_threads() -> int:
+    return int(_load_ref().ref_num_threads())

@@ -1,0 +1,61 @@
+#include "plan.hpp"
+
+#include <algorithm>
+
+namespace qsv {
+
+std::vector<Stage> plan_stages(const std::vector<Lowered>& gates, int n, int m,
+                               int low, int max_gates) {
+  std::vector<Stage> stages;
+  if (m > n) m = n;
+  if (low > m) low = m;
+  const uint64_t all = (n >= 64) ? ~0ull : ((1ull << n) - 1ull);
+  const uint64_t lowmask = (low >= 64) ? ~0ull : ((1ull << low) - 1ull);
+
+  std::vector<int> remaining;
+  remaining.reserve(gates.size());
+  for (int i = 0; i < (int)gates.size(); ++i)
+    if (gates[i].shape != SH_NONE) remaining.push_back(i);
+
+  std::vector<int> rest;
+  while (!remaining.empty()) {
+    uint64_t S = lowmask;
+    uint64_t blocked = 0;
+    Stage st;
+    rest.clear();
+    for (size_t r = 0; r < remaining.size(); ++r) {
+      const int gi = remaining[r];
+      const uint64_t b = gate_bits(gates[gi]);
+      const bool full = (max_gates > 0 && (int)st.gates.size() >= max_gates);
+      if (full || (b & blocked)) {
+        blocked |= b;
+        rest.push_back(gi);
+        continue;
+      }
+      if ((b & ~S) == 0) {
+        st.gates.push_back(gi);
+        continue;
+      }
+      if (__builtin_popcountll(S | b) <= m) {
+        S |= b;
+        st.gates.push_back(gi);
+        continue;
+      }
+      blocked |= b;
+      rest.push_back(gi);
+    }
+    // Fill the tile to exactly m bits (lowest unused bits first) so every
+    // stage of a plan moves tiles of the same size.
+    for (int b = 0; b < n && __builtin_popcountll(S) < m; ++b)
+      if (!((S >> b) & 1ull)) S |= 1ull << b;
+    S &= all;
+    st.m = 0;
+    for (int b = 0; b < n; ++b)
+      if ((S >> b) & 1ull) st.bits[st.m++] = b;
+    stages.push_back(std::move(st));
+    remaining.swap(rest);
+  }
+  return stages;
+}
+
+}  // namespace qsv

@@ -1,0 +1,52 @@
+// Fusion planner: groups a lowered gate list into stages.
+//
+// A stage owns a set S of m index bits (always including the L lowest bits,
+// so that every tile is made of contiguous runs of 2^L amplitudes).  The
+// state is streamed through shared memory one tile at a time -- a tile is
+// the 2^m amplitudes that agree on every bit outside S -- and all gates of
+// the stage, whose bits lie in S, are applied to the tile before it is
+// written back: one HBM read and write of the state per stage instead of
+// one per gate.
+//
+// Gates are taken greedily in circuit order.  A gate joins the current
+// stage if its bits are in S or can still be added to S (|S| <= m) and none
+// of its bits is "blocked"; a gate that cannot join blocks its bits, so no
+// later gate that shares a bit with it moves ahead of it.  Gates acting on
+// disjoint bits commute, so the stage order is a valid reordering of the
+// circuit.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+#include "lower.hpp"
+
+namespace qsv {
+
+struct Stage {
+  int m = 0;                  // tile bits
+  int bits[64];               // local bit j -> global bit (ascending)
+  std::vector<int> gates;     // indices into the lowered list, in order
+};
+
+inline uint64_t gate_bits(const Lowered& L) {
+  switch (L.shape) {
+    case SH_PAIR:
+    case SH_HALF:
+      return 1ull << L.t0;
+    case SH_QUAD:
+    case SH_CPAIR:
+    case SH_CHALF:
+    case SH_SWAP:
+      return (1ull << L.t0) | (1ull << L.t1);
+    default:
+      return 0;
+  }
+}
+
+// Builds stages for an n-qubit state with tiles of 2^m amplitudes whose
+// lowest `low` bits are contiguous.  max_gates bounds the gates of a stage
+// (0 = unbounded).
+std::vector<Stage> plan_stages(const std::vector<Lowered>& gates, int n, int m,
+                               int low, int max_gates);
+
+}  // namespace qsv

@@ -1,0 +1,189 @@
+"""GPU parity: the sm_100a kernels, called through the C ABI, against the
+reference's own outputs (golden fixtures), the CPU oracle, and each other.
+
+Tolerances:
+* reference-exact path (qsv_apply): bitwise equal (np.array_equal);
+* fused path (qsv_apply_fused): max-abs 1e-12 for complex128/float64 and
+  2e-5 for complex64/float32 on normalised states (the north-star bound is
+  1e-12 / 1e-5 at 30 qubits).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from cases import DTYPES, circuit_cases, gate_cases
+from make_golden import HERE
+from qclab_b200 import QsvError, StateVector, launch_count
+from qclab_b200 import _lib as L
+from qclab_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+GOLD = np.load(HERE / "reference_outputs.npz")
+
+
+def tol(dtype):
+    return 1e-12 if np.dtype(dtype) in (np.dtype(np.complex128), np.dtype(np.float64)) else 2e-5
+
+
+class States:
+    """One device state per (n, dtype), reused across cases."""
+
+    def __init__(self):
+        self.s = {}
+
+    def get(self, n, dtype):
+        k = (n, np.dtype(dtype))
+        if k not in self.s:
+            self.s[k] = StateVector(n, dtype)
+        return self.s[k]
+
+
+@pytest.fixture(scope="module")
+def states(cuda):
+    st = States()
+    yield st
+    for s in st.s.values():
+        s.close()
+
+
+def run_gpu(states, n, dtype, recs, op, off, x, fused=False, opts=None):
+    sv = states.get(n, dtype)
+    sv.upload(x)
+    sv.apply(recs, op, off, fused=fused, opts=opts)
+    return sv.download()
+
+
+@pytest.mark.parametrize("dtype", DTYPES, ids=lambda d: np.dtype(d).name)
+def test_every_gate_bitexact_vs_reference(states, dtype):
+    name = np.dtype(dtype).name
+    gold = GOLD[f"gates_{name}"]
+    pos = 0
+    before = launch_count()
+    for n, recs, op, off, x in gate_cases(dtype):
+        y = run_gpu(states, n, dtype, recs, op, off, x)
+        ref = gold[pos:pos + x.size]
+        pos += x.size
+        assert np.array_equal(y, ref), (name, n, recs[0]["kind"], op, np.max(np.abs(y - ref)))
+    assert pos == gold.size
+    assert launch_count() > before  # the CUDA kernels ran
+
+
+@pytest.mark.parametrize("dtype", DTYPES, ids=lambda d: np.dtype(d).name)
+def test_circuits_bitexact_vs_reference(states, dtype):
+    name = np.dtype(dtype).name
+    for cname, n, recs, op, off, x in circuit_cases(dtype):
+        y = run_gpu(states, n, dtype, recs, op, off, x)
+        assert np.array_equal(y, GOLD[f"circ_{name}_{cname}"]), cname
+
+
+@pytest.mark.parametrize("dtype", DTYPES, ids=lambda d: np.dtype(d).name)
+def test_fused_matches_reference_within_tolerance(states, dtype):
+    name = np.dtype(dtype).name
+    for cname, n, recs, op, off, x in circuit_cases(dtype):
+        xn = x / np.linalg.norm(x)
+        ref = oracle.apply(xn.astype(dtype), recs, op, off)
+        for opts in (None, L.FuseOpts(tile_bits=4, low_bits=2), L.FuseOpts(tile_bits=6, low_bits=1),
+                     L.FuseOpts(tile_bits=12, low_bits=5, max_stage_gates=3)):
+            y = run_gpu(states, n, dtype, recs, op, off, xn.astype(dtype), fused=True, opts=opts)
+            err = np.max(np.abs(y - ref))
+            assert err <= tol(dtype), (cname, opts and opts.tile_bits, err)
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=lambda d: np.dtype(d).name)
+@pytest.mark.parametrize("n", [13, 17, 21])
+def test_random_mixed_large(states, dtype, n):
+    """All gate classes at strides spanning lanes, registers and tiles."""
+    rng = np.random.default_rng(n)
+    c = W.random_mixed(n, 120, seed=n)
+    recs = c.gate_records(dtype)
+    x = (rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)).astype(dtype)
+    x /= np.linalg.norm(x)
+    for op in "NC":
+        ref = oracle.apply(x.copy(), recs, op)
+        y = run_gpu(states, n, dtype, recs, op, 0, x)
+        assert np.array_equal(y, ref)
+        yf = run_gpu(states, n, dtype, recs, op, 0, x, fused=True)
+        assert np.max(np.abs(yf - ref)) <= tol(dtype)
+
+
+def test_qft20_config(states):
+    """Plain QFT on 20 qubits, complex<double>, basis input from a seed."""
+    n = 20
+    recs = W.qft(n).gate_records(np.complex128)
+    assert len(recs) == 220
+    x = np.zeros(1 << n, dtype=np.complex128)
+    x[W.basis_index(n, seed=2024)] = 1
+    ref = oracle.apply(x.copy(), recs)
+    assert np.array_equal(run_gpu(states, n, np.complex128, recs, "N", 0, x), ref)
+    yf = run_gpu(states, n, np.complex128, recs, "N", 0, x, fused=True)
+    assert np.max(np.abs(yf - ref)) <= 1e-12
+
+
+def test_brick24_fused_vs_unfused(states):
+    n = 24
+    recs = W.brick(n, 6, seed=3).gate_records(np.complex128)
+    x = np.zeros(1 << n, dtype=np.complex128)
+    x[0] = 1
+    ref = oracle.apply(x.copy(), recs)
+    y = run_gpu(states, n, np.complex128, recs, "N", 0, x)
+    assert np.array_equal(y, ref)
+    yf = run_gpu(states, n, np.complex128, recs, "N", 0, x, fused=True)
+    assert np.max(np.abs(yf - ref)) <= 1e-12
+    assert abs(np.vdot(yf, yf).real - 1.0) < 1e-12
+
+
+def test_host_apply_entry_point(cuda):
+    """qsv_apply_host: the std::vector<T> drop-in (copy in, apply, copy out)."""
+    from qclab_b200 import QCircuit, Hadamard, CNOT
+    c = QCircuit(3)
+    c.push_back(Hadamard(0))
+    c.push_back(CNOT(0, 1))
+    c.push_back(CNOT(1, 2))
+    v = np.zeros(8, dtype=np.complex128)
+    v[0] = 1
+    c.simulate(v)
+    s = 1 / np.sqrt(2)
+    assert np.array_equal(v, np.array([s, 0, 0, 0, 0, 0, 0, s], dtype=np.complex128))
+    w = np.zeros(8, dtype=np.complex128)
+    w[0] = 1
+    c.simulate(w, fused=True)
+    assert np.max(np.abs(w - v)) < 1e-15
+
+
+def test_wrap_caller_owned_device_memory(cuda):
+    """simulate_device(T*): the library works in place on caller memory."""
+    import torch
+    from qclab_b200 import QCircuit, Hadamard
+    t = torch.zeros(16, dtype=torch.complex128, device="cuda")
+    t[0] = 1
+    sv = StateVector.wrap(t.data_ptr(), 4, np.complex128)
+    c = QCircuit(4)
+    for q in range(4):
+        c.push_back(Hadamard(q))
+    c.simulate_device(sv)
+    sv.synchronize()
+    assert torch.allclose(t.cpu(), torch.full((16,), 0.25, dtype=torch.complex128))
+    sv.close()
+
+
+def test_errors_are_reported_not_fatal(states):
+    from qclab_b200 import QCircuit, RotationX, CNOT
+    sv = states.get(3, np.float64)
+    c = QCircuit(3)
+    c.push_back(RotationX(0, 0.3))
+    with pytest.raises(QsvError) as e:
+        sv.apply(c.gate_records(np.float64))
+    assert e.value.status == 6
+    c2 = QCircuit(4)
+    c2.push_back(CNOT(0, 3))
+    with pytest.raises(QsvError) as e:
+        states.get(3, np.complex128).apply(c2.gate_records(np.complex128))
+    assert e.value.status == 2
+    short = np.zeros(4, dtype=np.complex128)
+    with pytest.raises(QsvError) as e:
+        states.get(3, np.complex128).upload_ptr(short.ctypes.data, short.nbytes)
+    assert e.value.status == 3
+    # the context is still usable
+    y = run_gpu(states, 3, np.complex128, c.gate_records(np.complex128), "N", 0,
+                np.eye(8, dtype=np.complex128)[0])
+    assert abs(np.vdot(y, y) - 1) < 1e-15
