@@ -173,6 +173,43 @@ qsv_status qsv_plan_stats(int nbQubits, qsv_dtype dtype, const qsv_gate* gates,
                           const qsv_fuse_opts* opts, int* nStages,
                           int* stage_gates, int capacity);
 
+/* ---- FP64 reductions (new: QCLAB++ has no observables) -------------------
+ * All sums accumulate in double precision whatever the state's dtype, with
+ * a deterministic two-stage reduction (per-CTA partials, then one fixed-order
+ * pass), so repeated calls give identical bits.
+ *
+ * Observables are sums of Pauli strings: `paulis` holds nTerms strings of
+ * nbQubits characters from {I,X,Y,Z}; character q of a term is the Pauli on
+ * qubit q (qubit 0 first, the QCLAB++ order).  coefs[t] is its real weight. */
+
+/* <psi|psi> */
+qsv_status qsv_norm2(qsv_state state, double* out);
+/* <a|b> as (re, im); a and b must have the same size and dtype. */
+qsv_status qsv_inner(qsv_state a, qsv_state b, double* out_re_im);
+/* <psi|H|psi> for H = sum_t coefs[t] * paulis[t]. */
+qsv_status qsv_expectation(qsv_state state, const char* paulis,
+                           const double* coefs, size_t nTerms, double* out);
+/* dst = H src (dst != src, same size and dtype; products formed in FP64). */
+qsv_status qsv_apply_observable(qsv_state dst, qsv_state src,
+                                const char* paulis, const double* coefs,
+                                size_t nTerms);
+
+/* ---- adjoint gradient (new: QCLAB++ has no differentiation) ---------------
+ * E(theta) = <psi|U^+ H U|psi> and dE/dtheta_p for every trainable angle:
+ * gates with param = p >= 0 (RotationX/Y/Z, RotationXX/YY/ZZ, CRotationX/Y/Z,
+ * Phase, CPhase; theta is the full angle of QRotation(theta)/QAngle(theta))
+ * contribute to grads[p]; gates sharing p add up.  One forward fused sweep,
+ * then one backward fused sweep that uncomputes psi and lambda = H psi with
+ * the inverse gates (no stored intermediate states).
+ *   state : psi on input; on return it holds psi again, recomputed by the
+ *           inverse gates (equal to the input up to rounding).
+ *   grads : nParams doubles (overwritten).     expval: E (may be NULL).
+ * Uses one extra state-sized work vector owned by the state object.        */
+qsv_status qsv_adjoint_gradient(qsv_state state, const qsv_gate* gates,
+                                size_t nGates, const char* paulis,
+                                const double* coefs, size_t nTerms,
+                                double* grads, int nParams, double* expval);
+
 /* Host-buffer convenience, the drop-in for QCircuit<T>::simulate(vector)
  * (include/qclab/QCircuit.hpp:164-166): copies `host` (2^nbQubits elements
  * of dtype) to the device, applies the gate list with `op`, copies back.

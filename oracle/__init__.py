@@ -175,3 +175,38 @@ def ref_apply(state: np.ndarray, recs, op: str = "N", offset: int = 0) -> np.nda
 
 def ref_threads() -> int:
     return int(_load_ref().ref_num_threads())
+
+
+# ---- FP64 reductions (host restatement, numpy) -----------------------------
+def pauli_apply(psi: np.ndarray, paulis: str) -> np.ndarray:
+    """P psi for a Pauli string (character q acts on qubit q = bit n-1-q)."""
+    N = psi.size
+    n = N.bit_length() - 1
+    f = zy = ny = 0
+    for q, c in enumerate(paulis):
+        b = 1 << (n - 1 - q)
+        if c == "X":
+            f |= b
+        elif c == "Y":
+            f |= b
+            zy |= b
+            ny += 1
+        elif c == "Z":
+            zy |= b
+    j = np.arange(N, dtype=np.uint64)
+    src = j ^ np.uint64(f)
+    sign = 1.0 - 2.0 * (np.bitwise_count(src & np.uint64(zy)) & 1).astype(np.float64)
+    return (1j ** ny) * sign * psi.astype(np.complex128)[src]
+
+
+def expectation(psi: np.ndarray, terms) -> float:
+    """sum_t c_t <psi|P_t|psi> in FP64; terms = [(coef, pauli string)]."""
+    x = psi.astype(np.complex128)
+    return float(sum(c * np.vdot(x, pauli_apply(x, p)).real for c, p in terms))
+
+
+def observable_apply(psi: np.ndarray, terms) -> np.ndarray:
+    out = np.zeros(psi.size, dtype=np.complex128)
+    for c, p in terms:
+        out += c * pauli_apply(psi, p)
+    return out

@@ -97,6 +97,12 @@ def _declare(lib):
         "qsv_plan_stats": ([i, i, gp, sz, C.c_char, i, p, C.POINTER(i), p, i], i),
         "qsv_apply_host": ([i, i, p, gp, sz, C.c_char, i, i], i),
         "qsv_last_stage_times": ([C.POINTER(C.c_float), i, C.POINTER(i)], i),
+        "qsv_norm2": ([p, C.POINTER(d)], i),
+        "qsv_inner": ([p, p, C.POINTER(d)], i),
+        "qsv_expectation": ([p, C.c_char_p, C.POINTER(d), sz, C.POINTER(d)], i),
+        "qsv_apply_observable": ([p, p, C.c_char_p, C.POINTER(d), sz], i),
+        "qsv_adjoint_gradient": ([p, gp, sz, C.c_char_p, C.POINTER(d), sz, C.POINTER(d), i,
+                                  C.POINTER(d)], i),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)

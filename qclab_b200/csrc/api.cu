@@ -34,6 +34,25 @@ qsv_status cuda_status(cudaError_t e, const char* what) {
 
 void count_launch(uint64_t k) { g_launches += k; }
 
+qsv_status ensure_aux(qsv_state_s* s, size_t bytes) {
+  if (s->aux_bytes >= bytes) return QSV_SUCCESS;
+  if (s->aux) {
+    qsv_status st = cuda_status(cudaStreamSynchronize(s->stream), "aux resize synchronize");
+    if (st) return st;
+    cudaFree(s->aux);
+    s->aux = nullptr;
+    s->aux_bytes = 0;
+  }
+  cudaError_t e = cudaMalloc(&s->aux, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    s->aux = nullptr;
+    return fail(QSV_ERROR_OUT_OF_MEMORY, "work-vector cudaMalloc of %zu bytes failed", bytes);
+  }
+  s->aux_bytes = bytes;
+  return QSV_SUCCESS;
+}
+
 qsv_status ensure_scratch(qsv_state_s* s, size_t bytes) {
   if (s->scratch_bytes >= bytes) return QSV_SUCCESS;
   if (s->scratch) {
@@ -193,10 +212,9 @@ qsv_status qsv_wrap(int nbQubits, qsv_dtype dtype, void* device_ptr, qsv_state* 
 qsv_status qsv_destroy(qsv_state s) {
   if (!s) return QSV_SUCCESS;
   qsv_status st = QSV_SUCCESS;
-  if (s->scratch) {
-    cudaStreamSynchronize(s->stream);
-    cudaFree(s->scratch);
-  }
+  if (s->scratch || s->aux) cudaStreamSynchronize(s->stream);
+  if (s->scratch) cudaFree(s->scratch);
+  if (s->aux) cudaFree(s->aux);
   if (s->owns && s->d) st = cuda_status(cudaFree(s->d), "cudaFree");
   delete s;
   return st;

@@ -2,6 +2,12 @@
 // shared memory once, one 2^m-amplitude tile per CTA, and applies all of the
 // stage's gates to the tile in shared memory.
 //
+// The same executor runs the adjoint's backward sweep: it then carries two
+// vectors (psi and lambda) through every tile, applies each inverse gate to
+// both, and evaluates the gradient terms w * Im(i^ny <lam| Pi P |psi>) of
+// the parametric gates inside the tile (one partial sum per tile, reduced
+// in a fixed order afterwards).
+//
 // Arithmetic here is FMA-contracted (within 1e-12 of the reference-exact
 // path for complex<double>, not bitwise: the planner reorders commuting
 // gates, which changes rounding).  Gates are specialised by the structure of
@@ -12,8 +18,10 @@
 #include <cstring>
 #include <vector>
 #include "common.cuh"
+#include "fused.hpp"
 #include "internal.hpp"
 #include "plan.hpp"
+#include "tile.cuh"
 
 namespace qsv {
 
@@ -35,15 +43,19 @@ struct FOp {
   int8_t j0, j1;   // local bits (PAIR/HALF/CPAIR/CHALF: j0 = target, j1 = control)
   int8_t cval;
   int8_t mul;
-  int16_t coef;    // index of the first coefficient
+  int8_t ny;       // SH_RED: number of Y factors
+  int8_t w;        // SH_RED: weight
+  int16_t coef;    // stage-relative index of the first coefficient
+  uint16_t f, zy, pm, pv;  // SH_RED: local masks
+  int32_t slot;    // SH_RED: row of the partial-sum matrix
 };
 
 struct StageArgs {
-  int n, m, low, nops;
-  int8_t bits[64];         // local bit -> global bit, ascending
+  TileArgs ta;
+  int nops;
   const FOp* ops;
   const void* coefs;
-  const uint64_t* runoff;  // 2^(m-low) global offsets of the tile's runs
+  double* partial;  // [slot][tile] partial sums of the SH_RED ops
 };
 
 __device__ __forceinline__ uint32_t ins0(uint32_t x, int p) {
@@ -117,7 +129,7 @@ __device__ __forceinline__ double mac(double acc, double c, double x) { return f
 __device__ __forceinline__ float mac(float acc, float c, float x) { return fmaf(c, x, acc); }
 
 template <typename V>
-__device__ __forceinline__ void apply_op(V* __restrict__ tile, int m, const FOp op,
+__device__ __forceinline__ void apply_op(V* __restrict__ tile, int m, const FOp& op,
                                          const V* __restrict__ cf) {
   const int tid = threadIdx.x, nthr = blockDim.x;
   switch (op.shape) {
@@ -201,36 +213,82 @@ __device__ __forceinline__ void apply_op(V* __restrict__ tile, int m, const FOp 
   }
 }
 
+// w * Im(i^ny * sum_{e in tile, (e & pm) == pv} conj(lam_e) (-1)^{pop((e^f)&zy)} psi_{e^f})
 template <typename V>
-__global__ void __launch_bounds__(512)
-k_stage(V* __restrict__ st, StageArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  V* tile = reinterpret_cast<V*>(smem_raw);
-  const int m = a.m, low = a.low;
-  const uint32_t size = 1u << m, lowmask = (1u << low) - 1u;
-  const uint64_t* __restrict__ runoff = a.runoff;
-  const V* __restrict__ coefs = static_cast<const V*>(a.coefs);
+__device__ __forceinline__ double red_op(const V* __restrict__ psi, const V* __restrict__ lam,
+                                         int m, const FOp& op) {
+  const uint32_t size = 1u << m;
+  double2 s = make_double2(0.0, 0.0);
+  for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) {
+    if ((e & op.pm) != op.pv) continue;
+    const uint32_t p = e ^ op.f;
+    const double sg = (__popc(p & op.zy) & 1) ? -1.0 : 1.0;
+    const double2 l = to_d2(lam[e]), x = to_d2(psi[p]);
+    s.x = fma(sg * l.x, x.x, fma(sg * l.y, x.y, s.x));
+    s.y = fma(sg * l.x, x.y, fma(-sg * l.y, x.x, s.y));
+  }
+  // Im(i^ny s)
+  double im;
+  switch (op.ny & 3) {
+    case 0: im = s.y; break;
+    case 1: im = s.x; break;
+    case 2: im = -s.y; break;
+    default: im = -s.x; break;
+  }
+  return op.w * im;
+}
 
-  // tile base: the block index spread over the bits outside the tile
-  uint64_t base = (uint64_t)blockIdx.x << low;
-  for (int j = low; j < m; ++j) base = insert_zero(base, a.bits[j]);
+template <typename V, int NV>
+__global__ void __launch_bounds__(512)
+k_stage(V* __restrict__ v0, V* __restrict__ v1, StageArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double2 red[32];
+  const int m = a.ta.m, low = a.ta.low;
+  const uint32_t size = 1u << m, lowmask = (1u << low) - 1u;
+  V* t0 = reinterpret_cast<V*>(smem_raw);
+  V* t1 = t0 + size;
+  const uint64_t* __restrict__ runoff = a.ta.runoff;
+  const V* __restrict__ coefs = static_cast<const V*>(a.coefs);
+  const uint64_t base = tile_base(a.ta, blockIdx.x);
 
 #pragma unroll 4
-  for (uint32_t e = threadIdx.x; e < size; e += blockDim.x)
-    tile[e] = st[base | runoff[e >> low] | (e & lowmask)];
+  for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) {
+    const uint64_t g = base | runoff[e >> low] | (e & lowmask);
+    t0[e] = v0[g];
+    if (NV == 2) t1[e] = v1[g];
+  }
   __syncthreads();
   for (int i = 0; i < a.nops; ++i) {
-    apply_op<V>(tile, m, a.ops[i], coefs);
+    const FOp op = a.ops[i];
+    if (op.shape == SH_RED) {
+      if (NV == 2) {
+        const double r = red_op<V>(t0, t1, m, op);
+        const double2 tot = block_sum(make_double2(r, 0.0), red);
+        if (threadIdx.x == 0) a.partial[(size_t)op.slot * gridDim.x + blockIdx.x] = tot.x;
+      }
+    } else {
+      apply_op<V>(t0, m, op, coefs);
+      if (NV == 2) apply_op<V>(t1, m, op, coefs);
+    }
     __syncthreads();
   }
 #pragma unroll 4
-  for (uint32_t e = threadIdx.x; e < size; e += blockDim.x)
-    st[base | runoff[e >> low] | (e & lowmask)] = tile[e];
+  for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) {
+    const uint64_t g = base | runoff[e >> low] | (e & lowmask);
+    v0[g] = t0[e];
+    if (NV == 2) v1[g] = t1[e];
+  }
 }
 
-// Default tile: 2^m amplitudes of 64 KB, runs of 2^low amplitudes >= 128 B.
-int default_tile_bits(size_t eb) { return eb >= 16 ? 12 : 13; }
-int default_low_bits(size_t eb) { return eb >= 16 ? 4 : 5; }
+// Fixed-order sum of each row of partial[rows][cols] (one block per row).
+__global__ void __launch_bounds__(256)
+k_rows(const double* __restrict__ partial, int cols, double* __restrict__ out) {
+  __shared__ double2 red[32];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < cols; i += blockDim.x) acc += partial[(size_t)blockIdx.x * cols + i];
+  const double2 s = block_sum(make_double2(acc, 0.0), red);
+  if (threadIdx.x == 0) out[blockIdx.x] = s.x;
+}
 
 int8_t classify(const Lowered& L, bool cplx) {
   if (L.shape != SH_PAIR && L.shape != SH_CPAIR) return F_GENERIC;
@@ -251,18 +309,22 @@ template <> double host_coef<double>(const double* m, int i) { return m[2 * i]; 
 template <> float host_coef<float>(const double* m, int i) { return (float)m[2 * i]; }
 
 template <typename V>
-qsv_status run_typed(qsv_state_s* s, const std::vector<Lowered>& gates, const qsv_fuse_opts* opts) {
+qsv_status execute_typed(const ExecArgs& x) {
   constexpr bool cplx = Elem<V>::cplx;
+  qsv_state_s* s = x.s;
   const int n = s->n;
-  int m = (opts && opts->tile_bits > 0) ? opts->tile_bits : default_tile_bits(sizeof(V));
+  const qsv_fuse_opts* opts = x.opts;
+  int m = (opts && opts->tile_bits > 0) ? opts->tile_bits : default_tile_bits(sizeof(V), x.nv);
   int low = (opts && opts->low_bits > 0) ? opts->low_bits : default_low_bits(sizeof(V));
   const int max_gates = (opts && opts->max_stage_gates > 0) ? opts->max_stage_gates : 256;
   if (m > 14) m = 14;
   if (m > n) m = n;
   if (low > m) low = m;
-  if ((size_t(1) << m) * sizeof(V) > 200 * 1024)
-    return fail(QSV_ERROR_SIZE, "tile of 2^%d elements exceeds shared memory", m);
+  const size_t smem = (size_t(1) << m) * sizeof(V) * x.nv;
+  if (smem > 200 * 1024)
+    return fail(QSV_ERROR_SIZE, "tile of %d x 2^%d elements exceeds shared memory", x.nv, m);
 
+  const std::vector<Lowered>& gates = *x.items;
   std::vector<Stage> stages = plan_stages(gates, n, m, low, max_gates);
   if (stages.empty()) return QSV_SUCCESS;
 
@@ -270,39 +332,49 @@ qsv_status run_typed(qsv_state_s* s, const std::vector<Lowered>& gates, const qs
   std::vector<FOp> ops;
   std::vector<V> coefs;
   std::vector<uint64_t> runoff;
-  struct Meta { size_t op0, nops, run0; };
+  struct Meta { size_t op0, nops, run0, coef0; };
   std::vector<Meta> meta;
-  const uint32_t nruns = 1u << (m - low);
   for (const Stage& stg : stages) {
-    Meta mt{ops.size(), stg.gates.size(), runoff.size()};
+    Meta mt{ops.size(), stg.gates.size(), runoff.size(), coefs.size()};
     int local_of[64];
     for (int j = 0; j < 64; ++j) local_of[j] = -1;
     for (int j = 0; j < stg.m; ++j) local_of[stg.bits[j]] = j;
+    auto local_mask = [&](uint64_t g) {
+      uint32_t r = 0;
+      for (int b = 0; b < n; ++b)
+        if ((g >> b) & 1ull) r |= 1u << local_of[b];
+      return (uint16_t)r;
+    };
     for (int gi : stg.gates) {
       const Lowered& L = gates[gi];
       FOp op{};
       op.shape = (int8_t)L.shape;
+      if (L.shape == SH_RED) {
+        op.f = local_mask(L.gen.f);
+        op.zy = local_mask(L.gen.zy);
+        op.pm = local_mask(L.gen.pm);
+        op.pv = local_mask(L.gen.pv);
+        op.ny = (int8_t)L.gen.ny;
+        op.w = (int8_t)L.gen.w;
+        op.slot = L.slot;
+        ops.push_back(op);
+        continue;
+      }
       op.form = classify(L, cplx);
       op.j0 = (int8_t)local_of[L.t0];
       op.j1 = (L.shape == SH_PAIR || L.shape == SH_HALF) ? 0 : (int8_t)local_of[L.t1];
       op.cval = (int8_t)L.cval;
       op.mul = (int8_t)L.mul;
-      if (coefs.size() > 30000) return fail(QSV_ERROR_SIZE, "fused plan too large");
-      op.coef = (int16_t)coefs.size();
+      // coefficient index relative to the stage's first coefficient
+      if (coefs.size() - mt.coef0 > 30000) return fail(QSV_ERROR_SIZE, "fused stage too large");
+      op.coef = (int16_t)(coefs.size() - mt.coef0);
       const int nc = (L.shape == SH_QUAD) ? 16 : (L.shape == SH_PAIR || L.shape == SH_CPAIR) ? 4 : 1;
       for (int i = 0; i < nc; ++i) coefs.push_back(host_coef<V>(L.m, i));
       ops.push_back(op);
     }
-    // run offsets: deposit the run index into the tile bits >= low
-    for (uint32_t r = 0; r < nruns; ++r) {
-      uint64_t off = 0;
-      for (int j = low; j < stg.m; ++j)
-        if ((r >> (j - low)) & 1u) off |= 1ull << stg.bits[j];
-      runoff.push_back(off);
-    }
+    tile_runoffs(stg.bits, stg.m, low, &runoff);
     meta.push_back(mt);
   }
-  // coefficient indices are per plan; ops index into one coefficient array
   const size_t ops_bytes = ops.size() * sizeof(FOp);
   const size_t coef_off = (ops_bytes + 255) & ~size_t(255);
   const size_t coef_bytes = coefs.size() * sizeof(V);
@@ -318,13 +390,16 @@ qsv_status run_typed(qsv_state_s* s, const std::vector<Lowered>& gates, const qs
                                                   s->stream), "fused plan upload"))
     return st;
 
-  const size_t smem = (size_t(1) << m) * sizeof(V);
+  auto kern = (x.nv == 2) ? k_stage<V, 2> : k_stage<V, 1>;
   if (qsv_status st = cuda_status(
-          cudaFuncSetAttribute(k_stage<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024),
+          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024),
           "fused stage shared-memory attribute"))
     return st;
   const int threads = std::min<int>(512, std::max<int>(32, (1 << m) / 8));
   const uint64_t ntiles = 1ull << (n - m);
+  if (x.ntiles_out) *x.ntiles_out = ntiles;
+  if (x.nslots > 0 && x.partial_bytes < (size_t)x.nslots * ntiles * sizeof(double))
+    return fail(QSV_ERROR_SIZE, "partial-sum buffer too small");
   const bool profile = opts && opts->profile;
   std::vector<cudaEvent_t> ev;
   if (profile) {
@@ -335,15 +410,17 @@ qsv_status run_typed(qsv_state_s* s, const std::vector<Lowered>& gates, const qs
   }
   for (size_t si = 0; si < stages.size(); ++si) {
     StageArgs a;
-    a.n = n;
-    a.m = stages[si].m;
-    a.low = low;
+    a.ta.n = n;
+    a.ta.m = stages[si].m;
+    a.ta.low = low;
+    for (int j = 0; j < 64; ++j) a.ta.bits[j] = (j < stages[si].m) ? (int8_t)stages[si].bits[j] : 0;
+    a.ta.runoff = reinterpret_cast<const uint64_t*>(dev + run_off) + meta[si].run0;
     a.nops = (int)meta[si].nops;
-    for (int j = 0; j < 64; ++j) a.bits[j] = (j < stages[si].m) ? (int8_t)stages[si].bits[j] : 0;
     a.ops = reinterpret_cast<const FOp*>(dev) + meta[si].op0;
-    a.coefs = dev + coef_off;
-    a.runoff = reinterpret_cast<const uint64_t*>(dev + run_off) + meta[si].run0;
-    k_stage<V><<<(unsigned)ntiles, threads, smem, s->stream>>>(static_cast<V*>(s->d), a);
+    a.coefs = dev + coef_off + meta[si].coef0 * sizeof(V);
+    a.partial = x.partial;
+    kern<<<(unsigned)ntiles, threads, smem, s->stream>>>(static_cast<V*>(x.v0),
+                                                         static_cast<V*>(x.v1), a);
     count_launch();
     if (qsv_status st = cuda_status(cudaGetLastError(), "fused stage launch")) return st;
     if (profile) cudaEventRecord(ev[si + 1], s->stream);
@@ -359,19 +436,36 @@ qsv_status run_typed(qsv_state_s* s, const std::vector<Lowered>& gates, const qs
     for (auto& e : ev) cudaEventDestroy(e);
     if (st) return st;
   }
+  if (x.nslots > 0) {
+    k_rows<<<x.nslots, 256, 0, s->stream>>>(x.partial, (int)ntiles, x.rows_out);
+    count_launch();
+    if (qsv_status st = cuda_status(cudaGetLastError(), "row reduction launch")) return st;
+  }
   return QSV_SUCCESS;
 }
 
 }  // namespace
 
-qsv_status run_fused(qsv_state_s* s, const std::vector<Lowered>& gates, const qsv_fuse_opts* opts) {
-  switch (s->dtype) {
-    case QSV_C128: return run_typed<double2>(s, gates, opts);
-    case QSV_C64:  return run_typed<float2>(s, gates, opts);
-    case QSV_F64:  return run_typed<double>(s, gates, opts);
-    case QSV_F32:  return run_typed<float>(s, gates, opts);
+int default_tile_bits(size_t eb, int nv) { return (eb >= 16 ? 12 : 13) - (nv == 2 ? 1 : 0); }
+int default_low_bits(size_t eb) { return eb >= 16 ? 4 : 5; }
+
+qsv_status execute_fused(const ExecArgs& x) {
+  switch (x.s->dtype) {
+    case QSV_C128: return execute_typed<double2>(x);
+    case QSV_C64:  return execute_typed<float2>(x);
+    case QSV_F64:  return execute_typed<double>(x);
+    case QSV_F32:  return execute_typed<float>(x);
   }
   return fail(QSV_ERROR_INVALID_VALUE, "bad dtype");
+}
+
+qsv_status run_fused(qsv_state_s* s, const std::vector<Lowered>& gates, const qsv_fuse_opts* opts) {
+  ExecArgs x;
+  x.s = s;
+  x.items = &gates;
+  x.v0 = s->d;
+  x.opts = opts;
+  return execute_fused(x);
 }
 
 }  // namespace qsv
@@ -399,7 +493,7 @@ extern "C" qsv_status qsv_plan_stats(int nbQubits, qsv_dtype dtype, const qsv_ga
   std::vector<Lowered> low;
   if (qsv_status st = lower_for_state(&fake, gates, nGates, op, offset, &low)) return st;
   const size_t eb = elem_bytes(dtype);
-  int m = (opts && opts->tile_bits > 0) ? opts->tile_bits : default_tile_bits(eb);
+  int m = (opts && opts->tile_bits > 0) ? opts->tile_bits : default_tile_bits(eb, 1);
   int lowb = (opts && opts->low_bits > 0) ? opts->low_bits : default_low_bits(eb);
   const int max_gates = (opts && opts->max_stage_gates > 0) ? opts->max_stage_gates : 256;
   std::vector<Stage> stages = plan_stages(low, nbQubits, std::min(m, 14), lowb, max_gates);

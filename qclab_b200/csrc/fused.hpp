@@ -1,0 +1,46 @@
+// Interface of the fused stage executor (apply_fused.cu).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+#include "internal.hpp"
+
+namespace qsv {
+
+struct ExecArgs {
+  qsv_state_s* s = nullptr;              // stream, size, dtype and plan scratch
+  const std::vector<Lowered>* items = nullptr;
+  void* v0 = nullptr;                    // vector the gates act on (psi)
+  void* v1 = nullptr;                    // second vector (lambda), nv == 2
+  int nv = 1;
+  const qsv_fuse_opts* opts = nullptr;
+  double* partial = nullptr;             // [nslots][ntiles] partial sums (SH_RED)
+  size_t partial_bytes = 0;
+  int nslots = 0;
+  double* rows_out = nullptr;            // nslots row sums (device)
+  uint64_t* ntiles_out = nullptr;
+};
+
+int default_tile_bits(size_t elem_bytes, int nv);
+int default_low_bits(size_t elem_bytes);
+
+// Plans the items into stages and runs them.
+qsv_status execute_fused(const ExecArgs& x);
+
+// Number of tiles the executor will use for nv vectors of a state.
+inline uint64_t fused_tiles(int n, size_t elem_bytes, int nv, const qsv_fuse_opts* opts) {
+  int m = (opts && opts->tile_bits > 0) ? opts->tile_bits : default_tile_bits(elem_bytes, nv);
+  if (m > 14) m = 14;
+  if (m > n) m = n;
+  return 1ull << (n - m);
+}
+
+// Tiled reductions (reduce.cu).
+qsv_status observable_internal(qsv_state_s* dst, qsv_state_s* src, const char* paulis,
+                               const double* coefs, size_t nterms);
+qsv_status inner_internal(qsv_state_s* a, qsv_state_s* b, double* out);
+qsv_status expectation_internal(qsv_state_s* s, const char* paulis, const double* coefs,
+                                size_t nterms, double* out);
+
+}  // namespace qsv

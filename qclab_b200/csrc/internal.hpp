@@ -17,6 +17,8 @@ struct qsv_state_s {
   cudaStream_t stream = nullptr;
   void* scratch = nullptr;  // device scratch owned by the state (plans, partial sums)
   size_t scratch_bytes = 0;
+  void* aux = nullptr;      // device work vectors (the adjoint's lambda and partials)
+  size_t aux_bytes = 0;
 };
 
 namespace qsv {
@@ -52,6 +54,7 @@ qsv_status lower_for_state(const qsv_state_s* s, const qsv_gate* gates,
 // Grows the state's device scratch buffer to at least `bytes` (stream-ordered
 // with respect to earlier work on the state's stream).
 qsv_status ensure_scratch(qsv_state_s* s, size_t bytes);
+qsv_status ensure_aux(qsv_state_s* s, size_t bytes);
 
 // Unfused launch of one lowered gate (reference-exact kernels).
 qsv_status launch_unfused(qsv_state_s* s, const Lowered& L);

@@ -32,7 +32,20 @@ namespace qsv {
 
 enum Shape : int {
   SH_NONE = 0, SH_PAIR = 1, SH_HALF = 2, SH_QUAD = 3,
-  SH_CPAIR = 4, SH_CHALF = 5, SH_SWAP = 6
+  SH_CPAIR = 4, SH_CHALF = 5, SH_SWAP = 6,
+  SH_RED = 7   // gradient reduction w * Im(i^ny <lam| Pi P |psi>) (adjoint sweep)
+};
+
+// Generator of a parametric gate for the adjoint gradient:
+// d/dtheta U(theta) = c * Pi * P * U with P a Pauli string (flip mask f,
+// sign mask zy, ny factors of Y) and Pi a projector onto index bits
+// (pm, pv).  dE/dtheta = w * Im(i^ny <lam| Pi P |psi>) with
+//   w = 1  for exp(-i theta/2 P) rotations (c = -i/2),
+//   w = -2 for Phase/CPhase (c = i, P = I, Pi onto the |1> target).
+struct Generator {
+  uint64_t f = 0, zy = 0, pm = 0, pv = 0;
+  int ny = 0;
+  int w = 1;
 };
 
 // One lowered gate.  Bit positions are amplitude-index bits (qubit q of an
@@ -50,7 +63,49 @@ struct Lowered {
   int param = -1;  // trainable parameter index of the source gate
   int kind = 0;    // source gate kind
   char op = 'N';
+  Generator gen;   // SH_RED: the generator to reduce
+  int slot = -1;   // SH_RED: output row
 };
+
+// Generator of gate g (qubits with offset) in an n-qubit register; returns
+// false if the gate kind has no trainable angle.
+inline bool generator_of(const qsv_gate& g, int offset, int n, Generator* out) {
+  Generator G;
+  auto bit = [n](int q) { return 1ull << (n - 1 - q); };
+  const uint64_t a = bit(g.qubit0 + offset);
+  switch (g.kind) {
+    case QSV_ROTATION_X: G.f = a; break;
+    case QSV_ROTATION_Y: G.f = a; G.zy = a; G.ny = 1; break;
+    case QSV_ROTATION_Z: G.zy = a; break;
+    case QSV_PHASE: G.pm = a; G.pv = a; G.w = -2; break;
+    case QSV_ROTATION_XX:
+    case QSV_ROTATION_YY:
+    case QSV_ROTATION_ZZ: {
+      const uint64_t ab = a | bit(g.qubit1 + offset);
+      if (g.kind == QSV_ROTATION_XX) G.f = ab;
+      if (g.kind == QSV_ROTATION_YY) { G.f = ab; G.zy = ab; G.ny = 2; }
+      if (g.kind == QSV_ROTATION_ZZ) G.zy = ab;
+      break;
+    }
+    case QSV_CROTATION_X:
+    case QSV_CROTATION_Y:
+    case QSV_CROTATION_Z:
+    case QSV_CPHASE: {
+      const uint64_t t = bit(g.qubit1 + offset);
+      G.pm = a;
+      G.pv = g.control_state ? a : 0;
+      if (g.kind == QSV_CROTATION_X) G.f = t;
+      if (g.kind == QSV_CROTATION_Y) { G.f = t; G.zy = t; G.ny = 1; }
+      if (g.kind == QSV_CROTATION_Z) G.zy = t;
+      if (g.kind == QSV_CPHASE) { G.pm |= t; G.pv |= t; G.w = -2; }
+      break;
+    }
+    default:
+      return false;
+  }
+  *out = G;
+  return true;
+}
 
 inline bool valid_op(char op) { return op == 'N' || op == 'T' || op == 'C'; }
 

@@ -38,6 +38,8 @@ inline uint64_t gate_bits(const Lowered& L) {
     case SH_CHALF:
     case SH_SWAP:
       return (1ull << L.t0) | (1ull << L.t1);
+    case SH_RED:
+      return L.gen.f | L.gen.zy | L.gen.pm;
     default:
       return 0;
   }

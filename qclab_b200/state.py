@@ -152,3 +152,46 @@ def apply_records(recs, op, nbQubits: int, vector, offset: int = 0, fused: bool 
 def launch_count() -> int:
     """Kernel launches issued by the library on this thread."""
     return int(L.load().qsv_launch_count())
+
+
+def _obs_args(obs):
+    from .observable import Observable
+    if not isinstance(obs, Observable):
+        raise TypeError("expected an Observable")
+    return obs.c_args()
+
+
+def _norm2(self) -> float:
+    out = C.c_double()
+    L.check(self._lib.qsv_norm2(self._h, C.byref(out)), "qsv_norm2")
+    return out.value
+
+
+def _inner(self, other: "StateVector") -> complex:
+    """<self|other> in FP64."""
+    out = (C.c_double * 2)()
+    L.check(self._lib.qsv_inner(self._h, other._h, out), "qsv_inner")
+    return complex(out[0], out[1])
+
+
+def _expectation(self, obs) -> float:
+    """<psi|H|psi> in FP64."""
+    buf, coefs, nt = _obs_args(obs)
+    if obs.nbQubits != self.nbQubits:
+        raise ValueError("observable size does not match the state")
+    out = C.c_double()
+    L.check(self._lib.qsv_expectation(self._h, buf, coefs, nt, C.byref(out)), "qsv_expectation")
+    return out.value
+
+
+def _apply_observable(self, src: "StateVector", obs) -> None:
+    """self = H src."""
+    buf, coefs, nt = _obs_args(obs)
+    L.check(self._lib.qsv_apply_observable(self._h, src._h, buf, coefs, nt),
+            "qsv_apply_observable")
+
+
+StateVector.norm2 = _norm2
+StateVector.inner = _inner
+StateVector.expectation = _expectation
+StateVector.apply_observable = _apply_observable

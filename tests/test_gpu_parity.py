@@ -119,6 +119,18 @@ def test_qft20_config(states):
     assert np.max(np.abs(yf - ref)) <= 1e-12
 
 
+def test_long_circuit_fused(states):
+    """A 12,300-gate plan: stage-relative coefficient indexing."""
+    n = 14
+    recs = W.brick(n, 600, seed=9).gate_records(np.complex128)
+    assert len(recs) > 12000
+    x = np.zeros(1 << n, dtype=np.complex128)
+    x[0] = 1
+    ref = oracle.apply(x.copy(), recs)
+    yf = run_gpu(states, n, np.complex128, recs, "N", 0, x, fused=True)
+    assert np.max(np.abs(yf - ref)) <= 1e-11
+
+
 def test_brick24_fused_vs_unfused(states):
     n = 24
     recs = W.brick(n, 6, seed=3).gate_records(np.complex128)

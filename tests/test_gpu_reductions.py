@@ -1,0 +1,93 @@
+"""FP64 reductions on the GPU against numpy (FP64) restatements."""
+import numpy as np
+import pytest
+
+import oracle
+from qclab_b200 import QsvError, StateVector
+from qclab_b200.observable import Observable, ising
+
+pytestmark = pytest.mark.gpu
+DTYPES = [np.complex128, np.complex64, np.float64, np.float32]
+
+
+def rand_state(n, dtype, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(size=1 << n) + (1j * rng.normal(size=1 << n) if np.dtype(dtype).kind == "c" else 0)
+    return (x / np.linalg.norm(x)).astype(dtype)
+
+
+def rand_observable(n, nterms, seed, allow_y=True):
+    rng = np.random.default_rng(seed)
+    H = Observable(n)
+    letters = "IXYZ" if allow_y else "IXZ"
+    for _ in range(nterms):
+        H.add(float(rng.normal()), "".join(rng.choice(list(letters), size=n)))
+    return H
+
+
+def rtol(dtype):
+    return 1e-12 if np.dtype(dtype) in (np.dtype(np.complex128), np.dtype(np.float64)) else 1e-6
+
+
+@pytest.mark.parametrize("dtype", DTYPES, ids=lambda d: np.dtype(d).name)
+@pytest.mark.parametrize("n", [1, 5, 13, 20])
+def test_norm_and_inner(cuda, dtype, n):
+    x, y = rand_state(n, dtype, 1), rand_state(n, dtype, 2)
+    with StateVector(n, dtype) as a, StateVector(n, dtype) as b:
+        a.upload(x)
+        b.upload(y)
+        x2, y2 = x.astype(np.complex128), y.astype(np.complex128)
+        ref = np.vdot(x2, y2)
+        assert abs(a.norm2() - np.vdot(x2, x2).real) < 1e-13
+        assert abs(a.inner(b) - ref) < 1e-13
+        assert a.norm2() == a.norm2()  # deterministic
+
+
+@pytest.mark.parametrize("dtype", DTYPES, ids=lambda d: np.dtype(d).name)
+@pytest.mark.parametrize("n", [2, 6, 14, 18])
+def test_expectation_random_pauli_sums(cuda, dtype, n):
+    x = rand_state(n, dtype, n)
+    H = rand_observable(n, 40, seed=n)
+    with StateVector(n, dtype) as a:
+        a.upload(x)
+        e = a.expectation(H)
+        ref = oracle.expectation(x, H.matrix_free_terms())
+        assert abs(e - ref) <= 1e-12 * max(1.0, abs(ref))
+        assert a.expectation(H) == e
+
+
+@pytest.mark.parametrize("n", [12, 24])
+def test_ising_expectation(cuda, n):
+    x = rand_state(n, np.complex128, 7)
+    H = ising(n)
+    assert len(H) == (n - 1) + n
+    with StateVector(n, np.complex128) as a:
+        a.upload(x)
+        assert abs(a.expectation(H) - oracle.expectation(x, H.matrix_free_terms())) < 1e-11
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=lambda d: np.dtype(d).name)
+@pytest.mark.parametrize("n", [3, 11, 17])
+def test_apply_observable(cuda, dtype, n):
+    x = rand_state(n, dtype, 3)
+    H = rand_observable(n, 25, seed=5)
+    with StateVector(n, dtype) as a, StateVector(n, dtype) as b:
+        a.upload(x)
+        b.apply_observable(a, H)
+        ref = oracle.observable_apply(x, H.matrix_free_terms())
+        tol = 1e-12 if dtype == np.complex128 else 1e-5
+        assert np.max(np.abs(b.download() - ref)) <= tol * max(1.0, np.max(np.abs(ref)))
+
+
+def test_reduction_errors(cuda):
+    with StateVector(3, np.float64) as a, StateVector(3, np.float64) as b:
+        H = Observable(3).add(1.0, "XYZ")
+        with pytest.raises(QsvError) as e:
+            b.apply_observable(a, H)
+        assert e.value.status == 6
+        H2 = Observable(3)
+        H2.paulis.append("XQZ")
+        H2.coefs.append(1.0)
+        with pytest.raises(QsvError) as e:
+            a.expectation(H2)
+        assert e.value.status == 1
