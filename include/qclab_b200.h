@@ -189,6 +189,27 @@ qsv_status qsv_inner(qsv_state a, qsv_state b, double* out_re_im);
 /* <psi|H|psi> for H = sum_t coefs[t] * paulis[t]. */
 qsv_status qsv_expectation(qsv_state state, const char* paulis,
                            const double* coefs, size_t nTerms, double* out);
+/* <psi|H|psi> like qsv_expectation, for callers that must not allocate
+ * device memory -- e.g. a host program or framework that has already
+ * reserved the GPU's memory for its own pool allocator (a cudaMalloc from
+ * this library would fail or fragment that pool), or a tight optimisation
+ * loop that cannot afford cudaMalloc/cudaFree, which synchronise the
+ * device.  No counterpart in the reference (QCLAB++ has no observables).
+ *   state       : caller-owned device array of 2^nbQubits elements of dtype.
+ *   cuda_stream : stream to run on (NULL = legacy default stream); the call
+ *                 synchronises it before returning.
+ * Calls no cudaMalloc/cudaFree: its work memory is a fixed 1 MiB array
+ * inside the library, held by every GPU that loads the library until the
+ * process exits.  An observable whose term table, run offsets and partial
+ * sums need more than 1 MiB is rejected with QSV_ERROR_SIZE (use
+ * qsv_expectation).  The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress, with the device current); make that
+ * first call before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU (other streams, other host threads) race.       */
+qsv_status qsv_expectation_noalloc(const void* state, int nbQubits,
+                                   qsv_dtype dtype, void* cuda_stream,
+                                   const char* paulis, const double* coefs,
+                                   size_t nTerms, double* out);
 /* dst = H src (dst != src, same size and dtype; products formed in FP64). */
 qsv_status qsv_apply_observable(qsv_state dst, qsv_state src,
                                 const char* paulis, const double* coefs,

@@ -521,3 +521,220 @@ qsv_status qsv_apply_observable(qsv_state dst, qsv_state src, const char* paulis
 }
 
 }  // extern "C"
+
+// ---- allocation-free expectation value --------------------------------------
+//
+// qsv_expectation_noalloc: the tiled expectation value above, for callers
+// that cannot allocate device memory.  Its work memory (term table, run
+// offsets, per-CTA partial sums, result) is the file-scope array below; the
+// CTAs loop over the tiles so the partial sums stay bounded whatever the
+// state size.
+#include <mutex>
+
+namespace qsv {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(1) << 20;  // 1 MiB per device
+constexpr unsigned kNoAllocBlocks = 148 * 4;
+constexpr int kNoAllocMaxDevices = 64;
+
+// Held by every GPU that loads this library, until process exit.  In host
+// code this name is only a stand-in for the symbol; kernels get the device
+// address obtained with cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device, looked up on
+// the first call per device (that device current).
+qsv_status noalloc_scratch(void** out) {
+  int dev = 0;
+  if (qsv_status st = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return st;
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return fail(QSV_ERROR_NOT_SUPPORTED, "device ordinal %d beyond %d", dev, kNoAllocMaxDevices);
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    if (qsv_status st = cuda_status(cudaGetSymbolAddress(&p, g_noalloc_scratch),
+                                    "cudaGetSymbolAddress(no-alloc scratch)"))
+      return st;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return QSV_SUCCESS;
+}
+
+// k_expect with the CTAs striding over tiles: one partial per CTA.
+template <typename V>
+__global__ void __launch_bounds__(kRedThreads)
+k_expect_tiles(const V* __restrict__ st, TileArgs ta, const DTerm* __restrict__ terms,
+               int nterms, uint64_t ntiles, double2* __restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* tile = reinterpret_cast<V*>(smem_raw);
+  __shared__ double2 red[32];
+  const uint32_t size = 1u << ta.m;
+  double2 acc = make_double2(0.0, 0.0);
+  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint64_t base = tile_base(ta, t);
+    __syncthreads();  // the previous tile is no longer read
+    for (uint32_t e = threadIdx.x; e < size; e += blockDim.x)
+      tile[e] = st[tile_global(ta, ta.runoff, base, e)];
+    __syncthreads();
+    for (int k = 0; k < nterms; ++k) {
+      const DTerm T = terms[k];
+      double2 s = make_double2(0.0, 0.0);
+      for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) {
+        const uint64_t g = tile_global(ta, ta.runoff, base, e);
+        const double2 x = to_d2(tile[e]);
+        const double2 y = to_d2(tile[e ^ T.flip_local]);
+        const double sg = sgn_of((g ^ T.flip) & T.zy);
+        s.x = fma(sg * x.x, y.x, fma(sg * x.y, y.y, s.x));
+        s.y = fma(sg * x.x, y.y, fma(-sg * x.y, y.x, s.y));
+      }
+      acc.x += T.wr * s.x - T.wi * s.y;
+      acc.y += T.wr * s.y + T.wi * s.x;
+    }
+  }
+  const double2 r = block_sum(acc, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = r;
+}
+
+template <typename V>
+qsv_status expect_noalloc_typed(const V* src, int n, cudaStream_t stream,
+                                const std::vector<HTerm>& T, double* out) {
+  if (T.empty()) {
+    *out = 0.0;
+    return QSV_SUCCESS;
+  }
+  const int m = std::min(n, sizeof(V) >= 16 ? 12 : 13);
+  const int low = std::min(m, sizeof(V) >= 16 ? 4 : 5);
+  std::vector<int> wide;
+  std::vector<Group> groups = group_terms(T, n, m, low, &wide);
+  for (const Group& G : groups)
+    if (G.m != m) return fail(QSV_ERROR_INVALID_VALUE, "internal: term group of %d bits", G.m);
+  const uint64_t N = dim(n);
+  const uint64_t ntiles = 1ull << (n - m);
+  const int nruns = 1 << (m - low);
+  const unsigned gblocks = (unsigned)std::min<uint64_t>(kNoAllocBlocks, ntiles);
+  const unsigned wblocks =
+      (unsigned)std::min<uint64_t>(kNoAllocBlocks, (N + kRedThreads - 1) / kRedThreads);
+  const size_t nparts = (size_t)gblocks * groups.size() + (size_t)wblocks * wide.size();
+  // layout: [partials double2][out double2][terms][runoffs]
+  const size_t out_off = nparts * sizeof(double2);
+  const size_t term_off = (out_off + sizeof(double2) + 255) & ~size_t(255);
+  const size_t term_bytes = T.size() * sizeof(DTerm);
+  const size_t run_off = (term_off + term_bytes + 255) & ~size_t(255);
+  const size_t total = run_off + groups.size() * (size_t)nruns * sizeof(uint64_t);
+  if (total > kNoAllocScratchBytes)
+    return fail(QSV_ERROR_SIZE,
+                "observable needs %zu bytes of work memory; the allocation-free entry point "
+                "has %zu (use qsv_expectation)", total, kNoAllocScratchBytes);
+  void* sp = nullptr;
+  if (qsv_status st = noalloc_scratch(&sp)) return st;
+  unsigned char* dev = static_cast<unsigned char*>(sp);
+
+  static const double pr[4] = {1, 0, -1, 0}, pi[4] = {0, 1, 0, -1};
+  std::vector<DTerm> dt;
+  std::vector<uint64_t> runoffs;
+  std::vector<size_t> term0;
+  for (const Group& G : groups) {
+    int local_of[64];
+    for (int j = 0; j < 64; ++j) local_of[j] = -1;
+    for (int j = 0; j < G.m; ++j) local_of[G.bits[j]] = j;
+    term0.push_back(dt.size());
+    for (int ti : G.terms) {
+      const HTerm& h = T[ti];
+      DTerm d{};
+      for (int b = 0; b < n; ++b)
+        if ((h.flip >> b) & 1ull) d.flip_local |= 1u << local_of[b];
+      d.flip = h.flip;
+      d.zy = h.zy;
+      d.wr = h.coef * pr[h.ny & 3];
+      d.wi = h.coef * pi[h.ny & 3];
+      dt.push_back(d);
+    }
+    tile_runoffs(G.bits, G.m, low, &runoffs);
+  }
+  std::vector<DTerm> wt;
+  for (int ti : wide) {
+    const HTerm& h = T[ti];
+    DTerm d{};
+    d.flip = h.flip;
+    d.zy = h.zy;
+    d.wr = h.coef * pr[h.ny & 3];
+    d.wi = h.coef * pi[h.ny & 3];
+    wt.push_back(d);
+  }
+  if (runoffs.size() != groups.size() * (size_t)nruns)
+    return fail(QSV_ERROR_INVALID_VALUE, "internal: run table size");
+  std::vector<unsigned char> host(total - term_off);
+  std::memcpy(host.data(), dt.data(), dt.size() * sizeof(DTerm));
+  std::memcpy(host.data() + (run_off - term_off), runoffs.data(), runoffs.size() * 8);
+  if (qsv_status st = cuda_status(cudaMemcpyAsync(dev + term_off, host.data(), host.size(),
+                                                  cudaMemcpyHostToDevice, stream),
+                                  "no-alloc observable upload"))
+    return st;
+  const size_t smem = (size_t(1) << m) * sizeof(V);
+  if (qsv_status st = cuda_status(cudaFuncSetAttribute((const void*)k_expect_tiles<V>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)smem), "no-alloc smem attribute"))
+    return st;
+  const int threads = std::min<int>(kRedThreads, std::max<int>(32, (1 << m) / 8));
+  double2* partial = reinterpret_cast<double2*>(dev);
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    TileArgs ta;
+    ta.n = n;
+    ta.m = groups[gi].m;
+    ta.low = low;
+    for (int j = 0; j < 64; ++j) ta.bits[j] = (j < ta.m) ? (int8_t)groups[gi].bits[j] : 0;
+    ta.runoff = reinterpret_cast<const uint64_t*>(dev + run_off) + gi * nruns;
+    const DTerm* terms = reinterpret_cast<const DTerm*>(dev + term_off) + term0[gi];
+    k_expect_tiles<V><<<gblocks, threads, smem, stream>>>(
+        src, ta, terms, (int)groups[gi].terms.size(), ntiles, partial + gi * gblocks);
+    count_launch();
+    if (qsv_status st = cuda_status(cudaGetLastError(), "no-alloc expectation launch")) return st;
+  }
+  for (size_t wi = 0; wi < wt.size(); ++wi) {
+    k_expect_wide<V><<<wblocks, kRedThreads, 0, stream>>>(
+        src, N, wt[wi], partial + (size_t)gblocks * groups.size() + wi * wblocks);
+    count_launch();
+    if (qsv_status st = cuda_status(cudaGetLastError(), "no-alloc wide-term launch")) return st;
+  }
+  double2* dout = reinterpret_cast<double2*>(dev + out_off);
+  k_final<<<1, 1024, 0, stream>>>(partial, (int)nparts, dout);
+  count_launch();
+  if (qsv_status st = cuda_status(cudaGetLastError(), "no-alloc final reduction")) return st;
+  double2 h;
+  if (qsv_status st = cuda_status(cudaMemcpyAsync(&h, dout, sizeof(h), cudaMemcpyDeviceToHost,
+                                                  stream), "no-alloc result copy"))
+    return st;
+  if (qsv_status st = cuda_status(cudaStreamSynchronize(stream), "no-alloc synchronize"))
+    return st;
+  *out = h.x;
+  return QSV_SUCCESS;
+}
+
+}  // namespace
+}  // namespace qsv
+
+extern "C" qsv_status qsv_expectation_noalloc(const void* state, int nbQubits, qsv_dtype dtype,
+                                              void* cuda_stream, const char* paulis,
+                                              const double* coefs, size_t nTerms, double* out) {
+  using namespace qsv;
+  if (!state) return fail(QSV_ERROR_INVALID_VALUE, "null state pointer");
+  if (!out) return fail(QSV_ERROR_INVALID_VALUE, "null output");
+  if (!dtype_valid(dtype)) return fail(QSV_ERROR_INVALID_VALUE, "bad dtype %d", (int)dtype);
+  if (nbQubits < 1 || nbQubits > kMaxQubits)
+    return fail(QSV_ERROR_SIZE, "nbQubits %d outside [1,%d]", nbQubits, kMaxQubits);
+  std::vector<HTerm> T;
+  if (qsv_status st = parse_terms(nbQubits, paulis, coefs, nTerms, &T)) return st;
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  switch (dtype) {
+    case QSV_C128: return expect_noalloc_typed<double2>((const double2*)state, nbQubits, stream, T, out);
+    case QSV_C64:  return expect_noalloc_typed<float2>((const float2*)state, nbQubits, stream, T, out);
+    case QSV_F64:  return expect_noalloc_typed<double>((const double*)state, nbQubits, stream, T, out);
+    case QSV_F32:  return expect_noalloc_typed<float>((const float*)state, nbQubits, stream, T, out);
+  }
+  return fail(QSV_ERROR_INVALID_VALUE, "bad dtype");
+}
