@@ -51,7 +51,10 @@ int run(const char* name, const qclab::QCircuit<T>& c, std::mt19937_64& rng, boo
       err = std::max(err, (double)std::abs(ref[i] - gpu[i]));
       same = same && (ref[i] == gpu[i]);
     }
-    const bool ok = fused ? err <= 1e-10 : same;
+    // fused sweeps reorder commuting gates: rounding-level differences on the
+    // unnormalised N(0,1) inputs (complex<double> 1e-10, complex<float> 5e-5)
+    const double tol = sizeof(qclab::real_t<T>) == 8 ? 1e-10 : 5e-5;
+    const bool ok = fused ? err <= tol : same;
     if (!ok) ++bad;
     std::printf("%-28s op=%c fused=%d max_abs=%.3e %s\n", name, opc, (int)fused, err,
                 ok ? "ok" : "FAIL");
