@@ -48,7 +48,89 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--unfused-gates", type=int, default=45)
+    p.add_argument("--parity-layers", type=int, default=10)
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the adjoint (24q) and precision (32q) measurements")
+    p.add_argument("--ps-params", type=int, default=24,
+                   help="parameters timed for the parameter-shift baseline")
     return p.parse_args()
+
+
+def adjoint_extra(torch, stream, ps_params):
+    """Adjoint gradient on the 24-qubit hardware-efficient ansatz (12 layers of
+    RotationY/RotationZ on every qubit + a CNOT ladder: 852 gates, 576
+    angles), complex<double>, H = sum Z_i Z_{i+1} + 0.5 sum X_i.  The GPU
+    parameter-shift baseline is timed on `ps_params` angles and extrapolated
+    to all 576 (each angle costs the same two simulations)."""
+    from qclab_b200 import StateVector
+    from qclab_b200 import workloads as W
+    from qclab_b200.gradients import adjoint_gradient, parameter_shift_gradient
+    from qclab_b200.observable import ising
+    n = 24
+    recs = W.hea(n, 12, seed=7).gate_records(np.complex128, number_params=True)
+    nparams = int(recs["param"].max()) + 1
+    H = ising(n)
+    with StateVector(n, np.complex128) as s:
+        s.set_stream(stream.cuda_stream)
+        for _ in range(2):
+            adjoint_gradient(s, recs, H)
+        torch.cuda.synchronize()
+        reps = 5
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            s.set_basis(0)
+            e, g = adjoint_gradient(s, recs, H)
+        b.record(stream)
+        torch.cuda.synchronize()
+        adj_ms = a.elapsed_time(b) / reps
+        s.set_basis(0)
+        subset = set(range(0, nparams, max(1, nparams // ps_params)))
+        parameter_shift_gradient(s, recs, H, params={0})  # warm-up
+        torch.cuda.synchronize()
+        a.record(stream)
+        ps = parameter_shift_gradient(s, recs, H, params=subset)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ps_ms = a.elapsed_time(b) * nparams / len(subset)
+    err = float(max(abs(g[p] - ps[p]) for p in subset))
+    return {"workload": "hea24_12layers_c128_ising", "gates": len(recs), "params": nparams,
+            "energy": e, "adjoint_ms": adj_ms, "grads_per_s": 1e3 / adj_ms,
+            "param_shift_ms_extrapolated": ps_ms, "param_shift_params_timed": len(subset),
+            "speedup_vs_param_shift": ps_ms / adj_ms, "max_abs_grad_diff_vs_param_shift": err}
+
+
+def precision_extra(torch, stream, n=32, depth=100, seed=11):
+    """Precision study: the brick generator at n qubits, depth `depth`, run in
+    complex<float> and complex<double> (fused), compared in FP64."""
+    from qclab_b200 import StateVector
+    from qclab_b200 import workloads as W
+    from qclab_b200.observable import Observable
+    circ = W.brick(n, depth, seed=seed)
+    r64, r128 = circ.gate_records(np.complex64), circ.gate_records(np.complex128)
+    zz = Observable(n).add(1.0, {0: "Z", 1: "Z"})
+    out = {"workload": f"brick{n}_depth{depth}", "gates": len(r128)}
+    with StateVector(n, np.complex128) as d, StateVector(n, np.complex64) as f:
+        d.set_stream(stream.cuda_stream)
+        f.set_stream(stream.cuda_stream)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        f.apply(r64, "N", 0, fused=True)
+        ev[1].record(stream)
+        d.apply(r128, "N", 0, fused=True)
+        ev[2].record(stream)
+        torch.cuda.synchronize()
+        ip, maxabs = f.compare(d)
+        zf, zd = f.expectation(zz), d.expectation(zz)
+        out.update({"c64_ms": ev[0].elapsed_time(ev[1]), "c128_ms": ev[1].elapsed_time(ev[2]),
+                    "c64_gates_per_s": len(r64) / (ev[0].elapsed_time(ev[1]) / 1e3),
+                    "c128_gates_per_s": len(r128) / (ev[1].elapsed_time(ev[2]) / 1e3),
+                    "c64_hbm_gbs_algorithmic": None,
+                    "infidelity": 1.0 - abs(ip) ** 2, "max_abs_error": maxabs,
+                    "zz01_c64": zf, "zz01_c128": zd, "zz01_error": abs(zf - zd),
+                    "norm_c64": f.norm2(), "norm_c128": d.norm2()})
+    return out
 
 
 def peaks():
@@ -315,6 +397,23 @@ def main():
         unf = {"gates": len(sub), "gates_per_s": len(sub) / (ums / 1e3),
                "hbm_gbs": unf_bytes / (ums / 1e3) / 1e9, "path": "qsv_apply (bit-exact)"}
 
+    # parity at full size: fused sweep vs the reference-exact per-gate path
+    # (bitwise equal to QCLAB++'s CPU apply in the tests) on the first layers
+    parity = None
+    if args.parity_layers > 0 and world == 1:
+        k = sum(n + len(range(l % 2, n - 1, 2)) for l in range(args.parity_layers))
+        sub = recs[:k]
+        ref_state = StateVector(n, np.complex128)
+        ref_state.set_stream(stream.cuda_stream)
+        ref_state.apply(sub, "N", 0, fused=False)
+        sv.set_basis(0)
+        sv.apply(sub, "N", 0, fused=True)
+        ip, maxabs = sv.compare(ref_state)
+        ref_state.close()
+        parity = {"gates": k, "layers": args.parity_layers, "max_abs_error": maxabs,
+                  "infidelity": 1.0 - abs(ip) ** 2,
+                  "against": "qsv_apply (bitwise equal to QCLAB++ CPU apply in tests)"}
+
     # end to end through the C ABI with host buffers (copies inside the timed region)
     e2e = None
     if not args.no_e2e:
@@ -354,6 +453,14 @@ def main():
         cpu = {"value": v, "unit": "gates/s", "cores": threads, "kind": kind, "sample": txt}
 
     sv.close()
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        for name, fn in (("adjoint", lambda: adjoint_extra(torch, stream, args.ps_params)),
+                         ("precision", lambda: precision_extra(torch, stream))):
+            try:
+                extras[name] = fn()
+            except Exception as ex:  # reported, not fatal: the headline line still prints
+                extras[name] = {"error": f"{type(ex).__name__}: {ex}"[:300]}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "gates/s", "n_gpus": world,
@@ -365,7 +472,9 @@ def main():
             "hbm_gbs_effective_unfused_equivalent": None,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": launches, "unfused_first_layer": unf,
+            "parity_vs_reference_exact": parity,
         }
+        line.update(extras)
         eff = 0
         for r in recs:
             k = int(r["kind"])

@@ -186,6 +186,11 @@ qsv_status qsv_plan_stats(int nbQubits, qsv_dtype dtype, const qsv_gate* gates,
 qsv_status qsv_norm2(qsv_state state, double* out);
 /* <a|b> as (re, im); a and b must have the same size and dtype. */
 qsv_status qsv_inner(qsv_state a, qsv_state b, double* out_re_im);
+/* Compares two states of the same size, possibly of different dtypes (the
+ * precision study: a complex<float> state against a complex<double> one):
+ * out[0], out[1] = <a|b> (re, im) and out[2] = max_j |a_j - b_j|, all in
+ * FP64.  Infidelity = 1 - |<a|b>|^2 for normalised states.               */
+qsv_status qsv_compare(qsv_state a, qsv_state b, double* out3);
 /* <psi|H|psi> for H = sum_t coefs[t] * paulis[t]. */
 qsv_status qsv_expectation(qsv_state state, const char* paulis,
                            const double* coefs, size_t nTerms, double* out);
@@ -230,6 +235,18 @@ qsv_status qsv_adjoint_gradient(qsv_state state, const qsv_gate* gates,
                                 size_t nGates, const char* paulis,
                                 const double* coefs, size_t nTerms,
                                 double* grads, int nParams, double* expval);
+
+/* ---- OpenQASM front end ----------------------------------------------------
+ * Parses OpenQASM text exactly as QCLAB++'s QASMFile does
+ * (include/qclab/io/QASMFile.hpp:42-167, src/io/QASMFile.cpp:16-53): gates
+ * h x y z rx ry rz p cx cy cz swap on one qreg, other commands skipped,
+ * angles read with stof/stod in dtype's precision.  Writes up to capacity
+ * records to gates (may be NULL to query), *count = gates parsed,
+ * *nbQubits = register size.  A command the reference cannot parse (e.g. an
+ * angle "pi/2") returns QSV_ERROR_INVALID_VALUE with the gates read so far,
+ * as the reference keeps them.                                             */
+qsv_status qsv_parse_qasm(const char* text, qsv_dtype dtype, qsv_gate* gates,
+                          size_t capacity, size_t* count, int* nbQubits);
 
 /* Host-buffer convenience, the drop-in for QCircuit<T>::simulate(vector)
  * (include/qclab/QCircuit.hpp:164-166): copies `host` (2^nbQubits elements

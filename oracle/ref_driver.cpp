@@ -238,6 +238,33 @@ void* ref_circuit_create(int n, int dtype, const qsv_gate* gates, size_t count, 
 
 void ref_circuit_destroy(void* c) { delete static_cast<AnyCircuit*>(c); }
 
+// QCircuit<T>(filename): the reference's own OpenQASM reader
+// (include/qclab/QCircuit.hpp:82-93).
+void* ref_circuit_from_qasm(const char* filename, int dtype, int* nbQubits) {
+  switch (dtype) {
+    case QSV_C128: {
+      auto c = std::make_shared<qclab::QCircuit<std::complex<double>>>(std::string(filename));
+      *nbQubits = c->nbQubits();
+      return new AnyCircuit{dtype, c};
+    }
+    case QSV_C64: {
+      auto c = std::make_shared<qclab::QCircuit<std::complex<float>>>(std::string(filename));
+      *nbQubits = c->nbQubits();
+      return new AnyCircuit{dtype, c};
+    }
+  }
+  return nullptr;
+}
+
+int ref_circuit_nb_gates(void* c) {
+  auto* ac = static_cast<AnyCircuit*>(c);
+  if (ac->dtype == QSV_C128)
+    return (int)static_cast<qclab::QCircuit<std::complex<double>>*>(ac->c.get())->nbGates();
+  if (ac->dtype == QSV_C64)
+    return (int)static_cast<qclab::QCircuit<std::complex<float>>*>(ac->c.get())->nbGates();
+  return -1;
+}
+
 void* ref_vec_create(int dtype, uint64_t count) {
   auto* av = new AnyVec{dtype, nullptr, nullptr};
   switch (dtype) {

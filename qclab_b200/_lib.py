@@ -102,6 +102,8 @@ def _declare(lib):
         "qsv_expectation": ([p, C.c_char_p, C.POINTER(d), sz, C.POINTER(d)], i),
         "qsv_apply_observable": ([p, p, C.c_char_p, C.POINTER(d), sz], i),
         "qsv_expectation_noalloc": ([p, i, i, p, C.c_char_p, C.POINTER(d), sz, C.POINTER(d)], i),
+        "qsv_compare": ([p, p, C.POINTER(d)], i),
+        "qsv_parse_qasm": ([C.c_char_p, i, p, sz, C.POINTER(sz), C.POINTER(i)], i),
         "qsv_adjoint_gradient": ([p, gp, sz, C.c_char_p, C.POINTER(d), sz, C.POINTER(d), i,
                                   C.POINTER(d)], i),
     }

@@ -58,4 +58,38 @@ std::vector<Stage> plan_stages(const std::vector<Lowered>& gates, int n, int m,
   return stages;
 }
 
+std::vector<Pass> plan_passes(const std::vector<uint32_t>& op_bits, int m, int r) {
+  std::vector<Pass> passes;
+  std::vector<int> remaining(op_bits.size()), rest;
+  for (size_t i = 0; i < op_bits.size(); ++i) remaining[i] = (int)i;
+  while (!remaining.empty()) {
+    uint32_t S = 0, blocked = 0;
+    Pass p;
+    rest.clear();
+    for (int oi : remaining) {
+      const uint32_t b = op_bits[oi];
+      if (b & blocked) {
+        blocked |= b;
+        rest.push_back(oi);
+        continue;
+      }
+      if ((b & ~S) == 0 || __builtin_popcount(S | b) <= r) {
+        S |= b;
+        p.ops.push_back(oi);
+        continue;
+      }
+      blocked |= b;
+      rest.push_back(oi);
+    }
+    for (int j = 0; j < m && __builtin_popcount(S) < r; ++j)
+      if (!((S >> j) & 1u)) S |= 1u << j;
+    p.r = 0;
+    for (int j = 0; j < m; ++j)
+      if ((S >> j) & 1u) p.pos[p.r++] = j;
+    passes.push_back(std::move(p));
+    remaining.swap(rest);
+  }
+  return passes;
+}
+
 }  // namespace qsv

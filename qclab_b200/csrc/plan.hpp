@@ -51,4 +51,19 @@ inline uint64_t gate_bits(const Lowered& L) {
 std::vector<Stage> plan_stages(const std::vector<Lowered>& gates, int n, int m,
                                int low, int max_gates);
 
+// A register pass inside a stage: r tile bits (ascending local positions)
+// whose 2^r amplitudes one thread holds in registers while it applies the
+// pass's ops (indices into the stage's op list, in order).
+struct Pass {
+  int r = 0;
+  int pos[8];
+  std::vector<int> ops;
+};
+
+// Groups a stage's ops (given by their local bit masks, in order) into
+// register passes of at most r bits, with the same blocking rule as
+// plan_stages, so each pass is a valid reordering of commuting ops.  Every
+// pass is padded to exactly r bits (the lowest unused local bits; m >= r).
+std::vector<Pass> plan_passes(const std::vector<uint32_t>& op_bits, int m, int r);
+
 }  // namespace qsv

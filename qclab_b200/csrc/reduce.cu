@@ -421,6 +421,98 @@ qsv_status check(qsv_state s) {
   return QSV_SUCCESS;
 }
 
+// <a|b> and max |a_j - b_j| for states of possibly different element types.
+template <typename VA, typename VB>
+__global__ void __launch_bounds__(kRedThreads)
+k_compare(const VA* __restrict__ a, const VB* __restrict__ b, uint64_t N,
+          double2* __restrict__ partial, double* __restrict__ pmax) {
+  __shared__ double2 red[32];
+  __shared__ double mx[32];
+  double2 acc = make_double2(0.0, 0.0);
+  double m = 0.0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < N;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const double2 x = to_d2(a[i]), y = to_d2(b[i]);
+    acc.x = fma(x.x, y.x, fma(x.y, y.y, acc.x));
+    acc.y = fma(x.x, y.y, fma(-x.y, y.x, acc.y));
+    const double dx = x.x - y.x, dy = x.y - y.y;
+    m = fmax(m, sqrt(fma(dx, dx, dy * dy)));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) mx[threadIdx.x >> 5] = m;
+  const double2 s = block_sum(acc, red);  // synchronises the block
+  if (threadIdx.x == 0) {
+    double bm = 0.0;
+    for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) bm = fmax(bm, mx[w]);
+    partial[blockIdx.x] = s;
+    pmax[blockIdx.x] = bm;
+  }
+}
+
+__global__ void k_max(const double* __restrict__ v, int count, double* __restrict__ out) {
+  __shared__ double mx[32];
+  double m = 0.0;
+  for (int i = threadIdx.x; i < count; i += blockDim.x) m = fmax(m, v[i]);
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) mx[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double bm = 0.0;
+    for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) bm = fmax(bm, mx[w]);
+    *out = bm;
+  }
+}
+
+template <typename VA, typename VB>
+qsv_status compare_typed(qsv_state_s* a, qsv_state_s* b, double* out) {
+  const uint64_t N = dim(a->n);
+  const unsigned blocks = (unsigned)std::min<uint64_t>(kRedBlocks, (N + kRedThreads - 1) / kRedThreads);
+  const size_t bytes = (blocks + 1) * sizeof(double2) + (blocks + 1) * sizeof(double);
+  if (qsv_status st = ensure_scratch(a, bytes)) return st;
+  double2* partial = static_cast<double2*>(a->scratch);
+  double* pmax = reinterpret_cast<double*>(partial + blocks + 1);
+  k_compare<VA, VB><<<blocks, kRedThreads, 0, a->stream>>>(
+      static_cast<const VA*>(a->d), static_cast<const VB*>(b->d), N, partial, pmax);
+  k_final<<<1, 1024, 0, a->stream>>>(partial, (int)blocks, partial + blocks);
+  k_max<<<1, 1024, 0, a->stream>>>(pmax, (int)blocks, pmax + blocks);
+  count_launch(3);
+  if (qsv_status st = cuda_status(cudaGetLastError(), "compare launch")) return st;
+  double2 h;
+  double hm;
+  if (qsv_status st = cuda_status(cudaMemcpyAsync(&h, partial + blocks, sizeof(h),
+                                                  cudaMemcpyDeviceToHost, a->stream), "compare copy"))
+    return st;
+  if (qsv_status st = cuda_status(cudaMemcpyAsync(&hm, pmax + blocks, sizeof(hm),
+                                                  cudaMemcpyDeviceToHost, a->stream), "compare copy"))
+    return st;
+  if (qsv_status st = cuda_status(cudaStreamSynchronize(a->stream), "compare synchronize")) return st;
+  out[0] = h.x;
+  out[1] = h.y;
+  out[2] = hm;
+  return QSV_SUCCESS;
+}
+
+template <typename VA>
+qsv_status compare_b(qsv_state_s* a, qsv_state_s* b, double* out) {
+  switch (b->dtype) {
+    case QSV_C128: return compare_typed<VA, double2>(a, b, out);
+    case QSV_C64:  return compare_typed<VA, float2>(a, b, out);
+    case QSV_F64:  return compare_typed<VA, double>(a, b, out);
+    case QSV_F32:  return compare_typed<VA, float>(a, b, out);
+  }
+  return fail(QSV_ERROR_INVALID_VALUE, "bad dtype");
+}
+
+qsv_status compare_dispatch(qsv_state_s* a, qsv_state_s* b, double* out) {
+  switch (a->dtype) {
+    case QSV_C128: return compare_b<double2>(a, b, out);
+    case QSV_C64:  return compare_b<float2>(a, b, out);
+    case QSV_F64:  return compare_b<double>(a, b, out);
+    case QSV_F32:  return compare_b<float>(a, b, out);
+  }
+  return fail(QSV_ERROR_INVALID_VALUE, "bad dtype");
+}
+
 }  // namespace
 
 qsv_status expectation_internal(qsv_state_s* s, const char* paulis, const double* coefs,
@@ -504,6 +596,17 @@ qsv_status qsv_expectation(qsv_state s, const char* paulis, const double* coefs,
   if (qsv_status st = check(s)) return st;
   if (!out) return fail(QSV_ERROR_INVALID_VALUE, "null output");
   return expectation_internal(s, paulis, coefs, nterms, out);
+}
+
+qsv_status qsv_compare(qsv_state a, qsv_state b, double* out) {
+  if (qsv_status st = check(a)) return st;
+  if (qsv_status st = check(b)) return st;
+  if (!out) return fail(QSV_ERROR_INVALID_VALUE, "null output");
+  if (a->n != b->n) return fail(QSV_ERROR_SIZE, "qsv_compare: states differ in size");
+  if (b->stream != a->stream)
+    if (qsv_status st = cuda_status(cudaStreamSynchronize(b->stream), "compare stream sync"))
+      return st;
+  return compare_dispatch(a, b, out);
 }
 
 qsv_status qsv_apply_observable(qsv_state dst, qsv_state src, const char* paulis,

@@ -191,6 +191,14 @@ def _apply_observable(self, src: "StateVector", obs) -> None:
             "qsv_apply_observable")
 
 
+def _compare(self, other: "StateVector"):
+    """(<self|other>, max_j |self_j - other_j|) in FP64; dtypes may differ."""
+    out = (C.c_double * 3)()
+    L.check(self._lib.qsv_compare(self._h, other._h, out), "qsv_compare")
+    return complex(out[0], out[1]), out[2]
+
+
+StateVector.compare = _compare
 StateVector.norm2 = _norm2
 StateVector.inner = _inner
 StateVector.expectation = _expectation
