@@ -184,6 +184,10 @@ qsv_status qsv_plan_stats(int nbQubits, qsv_dtype dtype, const qsv_gate* gates,
 
 /* <psi|psi> */
 qsv_status qsv_norm2(qsv_state state, double* out);
+/* psi /= sqrt(<psi|psi>) with the norm formed in FP64 (removes the norm
+ * drift that rounding leaves in long complex<float> sweeps); *norm2_out
+ * (may be NULL) receives <psi|psi> before the scaling. */
+qsv_status qsv_normalize(qsv_state state, double* norm2_out);
 /* <a|b> as (re, im); a and b must have the same size and dtype. */
 qsv_status qsv_inner(qsv_state a, qsv_state b, double* out_re_im);
 /* Compares two states of the same size, possibly of different dtypes (the
@@ -235,6 +239,60 @@ qsv_status qsv_adjoint_gradient(qsv_state state, const qsv_gate* gates,
                                 size_t nGates, const char* paulis,
                                 const double* coefs, size_t nTerms,
                                 double* grads, int nParams, double* expval);
+
+/* ---- batched variational sweeps (new: no reference counterpart) ------------
+ * Many independent circuits, each with its own qubit count (5..30), gate
+ * list and Pauli-sum observable: energy E_c = <psi_c|H_c|psi_c> from |0...0>
+ * and the full adjoint gradient dE_c/dtheta_p of every circuit, computed by
+ * ONE persistent kernel launch (a CTA per circuit at a time, largest
+ * circuits first; circuits whose two work vectors fit a CTA's shared memory
+ * never touch HBM) that qsv_batch_run can capture in a CUDA graph.
+ *   gates + gate_offsets[c..c+1]     : circuit c's records (param >= 0 marks
+ *                                      a trainable angle, < nParams[c])
+ *   paulis/coefs + term_offsets[c..] : circuit c's terms (nbQubits[c] chars
+ *                                      each, strings back to back)
+ * Results: energies[nCircuits], gradients concatenated in circuit order.  */
+typedef struct qsv_batch_s* qsv_batch;
+typedef struct qsv_batch_opts {
+  int tile_bits;     /* 2^m amplitudes per shared-memory tile (0 = default) */
+  int low_bits;      /* contiguous low bits of a tile (0 = default)          */
+  int ctas_per_sm;   /* cap on resident CTAs per SM (0 = occupancy limit)   */
+  int reserved[5];
+} qsv_batch_opts;
+qsv_status qsv_batch_create(qsv_dtype dtype, int nCircuits, const int* nbQubits,
+                            const qsv_gate* gates, const size_t* gate_offsets,
+                            const char* paulis, const double* coefs,
+                            const size_t* term_offsets, const int* nParams,
+                            const qsv_batch_opts* opts, qsv_batch* out);
+/* One launch of the whole batch on cuda_stream; use_graph != 0 captures it
+ * (results reset + persistent kernel) in a CUDA graph on first use and
+ * replays the graph afterwards. */
+qsv_status qsv_batch_run(qsv_batch batch, void* cuda_stream, int use_graph);
+qsv_status qsv_batch_results(qsv_batch batch, void* cuda_stream,
+                             double* energies, double* gradients);
+qsv_status qsv_batch_info(qsv_batch batch, int* blocks, int* threads,
+                          int* tile_bits, size_t* workspace_bytes);
+qsv_status qsv_batch_destroy(qsv_batch batch);
+
+/* ---- unitaries ---------------------------------------------------------------
+ * A 2^n x 2^n matrix lives on the device in a state object of 2n qubits
+ * (qsv_create(2n, ...)) holding its entries column-major -- (r, c) at
+ * r + c 2^n, the layout of qclab::dense::SquareMatrix.  Gates address the n
+ * matrix qubits.                                                             */
+/* qclab::dense::eye: the identity, the start of QCircuit::matrix()
+ * (include/qclab/QCircuit.hpp:120-126).  QSV_ERROR_SIZE for an odd count. */
+qsv_status qsv_set_identity(qsv_state matrix);
+/* QObject<T>::apply(Side side, Op op, nbQubits, SquareMatrix<T>&, offset)
+ * for a gate list in circuit order (include/qclab/QCircuit.hpp:176-204;
+ * per gate src/qgates/QGate1.cpp:27-80, QGate2.cpp, QControlledGate2.cpp):
+ * side 'R' gives matrix <- op(U) matrix, side 'L' matrix <- matrix op(U).
+ * fused != 0 runs the fused stage sweep, else the per-gate kernels.       */
+qsv_status qsv_apply_matrix(qsv_state matrix, const qsv_gate* gates, size_t nGates,
+                            char side, char op, int offset, int fused);
+/* qclab::nrmF (include/qclab/QCircuit.hpp:407-430): scale * sqrt(sum
+ * |(a - b) / scale|^2) with scale = max |a - b| (1 if zero), in FP64, for
+ * two objects of the same size (any element types).                      */
+qsv_status qsv_nrmF(qsv_state a, qsv_state b, double* out);
 
 /* ---- OpenQASM front end ----------------------------------------------------
  * Parses OpenQASM text exactly as QCLAB++'s QASMFile does

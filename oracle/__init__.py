@@ -115,6 +115,13 @@ def _load_ref():
             lib.ref_vec_destroy.argtypes = [C.c_void_p]
             lib.ref_circuit_apply.argtypes = [C.c_void_p, C.c_void_p, C.c_char, C.c_int]
             lib.ref_circuit_apply.restype = C.c_int
+            lib.ref_circuit_apply_side.argtypes = [C.c_void_p, C.c_char, C.c_char, C.c_int,
+                                                   C.c_int, C.c_void_p]
+            lib.ref_circuit_apply_side.restype = C.c_int
+            lib.ref_circuit_matrix.argtypes = [C.c_void_p, C.c_void_p]
+            lib.ref_circuit_matrix.restype = C.c_int
+            lib.ref_nrmF.argtypes = [C.c_void_p, C.c_void_p]
+            lib.ref_nrmF.restype = C.c_double
             lib.ref_num_threads.restype = C.c_int
             lib.ref_set_num_threads.argtypes = [C.c_int]
             _ref = lib
@@ -171,6 +178,50 @@ def ref_apply(state: np.ndarray, recs, op: str = "N", offset: int = 0) -> np.nda
     out = rc.state.copy()
     rc.close()
     return out
+
+
+def ref_matrix(n: int, dtype, recs) -> np.ndarray:
+    """The reference's ``QCircuit<T>::matrix()`` of a record list."""
+    rc = RefCircuit(n, dtype, recs)
+    out = np.zeros((1 << n) * (1 << n), dtype=rc.dtype)
+    st = rc.lib.ref_circuit_matrix(rc.c, out.ctypes.data)
+    rc.close()
+    if st:
+        raise RuntimeError(f"reference matrix failed ({st})")
+    return out.reshape(1 << n, 1 << n, order="F")
+
+
+def ref_apply_side(matrix: np.ndarray, recs, side: str, op: str, nbq: int, offset: int = 0,
+                   circuit_qubits: int | None = None) -> np.ndarray:
+    """The reference's ``QCircuit<T>::apply(side, op, nbq, matrix, offset)``
+    on a copy of ``matrix`` (the circuit has ``circuit_qubits`` qubits)."""
+    rc = RefCircuit(circuit_qubits or nbq, matrix.dtype, recs)
+    buf = np.ascontiguousarray(matrix.flatten(order="F"))
+    st = rc.lib.ref_circuit_apply_side(rc.c, side.encode(), op.encode(), nbq, offset,
+                                       buf.ctypes.data)
+    rc.close()
+    if st:
+        raise RuntimeError(f"reference apply(side) failed ({st})")
+    return buf.reshape(matrix.shape, order="F")
+
+
+def ref_nrmF(n: int, dtype, recs1, recs2) -> float:
+    """The reference's ``qclab::nrmF`` of two record lists."""
+    a, b = RefCircuit(n, dtype, recs1), RefCircuit(n, dtype, recs2)
+    v = float(a.lib.ref_nrmF(a.c, b.c))
+    a.close()
+    b.close()
+    return v
+
+
+def nrmF(m1: np.ndarray, m2: np.ndarray) -> float:
+    """numpy restatement of qclab::nrmF (include/qclab/QCircuit.hpp:407-430)
+    on two matrices: scale = max |m1 - m2| (1 if 0), FP64."""
+    d = m1.astype(np.complex128) - m2.astype(np.complex128)
+    scale = float(np.max(np.abs(d))) if d.size else 0.0
+    if scale == 0.0:
+        scale = 1.0
+    return scale * float(np.sqrt(np.sum((d.real / scale) ** 2 + (d.imag / scale) ** 2)))
 
 
 def ref_threads() -> int:

@@ -218,6 +218,39 @@ int run(AnyCircuit* ac, AnyVec* av, char op, int offset) {
   return 0;
 }
 
+// QCircuit<T>::apply(side, op, nbQubits, SquareMatrix<T>&, offset)
+// (include/qclab/QCircuit.hpp:176-204) on a caller-held column-major matrix.
+template <typename T>
+int run_side(AnyCircuit* ac, char side, char op, int nbq, int offset, void* data) {
+  auto* c = static_cast<qclab::QCircuit<T>*>(ac->c.get());
+  const int64_t N = int64_t(1) << nbq;
+  T* d = static_cast<T*>(data);
+  qclab::dense::SquareMatrix<T> M(N);
+  for (int64_t j = 0; j < N; ++j)
+    for (int64_t i = 0; i < N; ++i) M(i, j) = d[i + j * N];
+  c->apply(static_cast<qclab::Side>(side), static_cast<qclab::Op>(op), nbq, M, offset);
+  for (int64_t j = 0; j < N; ++j)
+    for (int64_t i = 0; i < N; ++i) d[i + j * N] = M(i, j);
+  return 0;
+}
+
+// QCircuit<T>::matrix() (include/qclab/QCircuit.hpp:120-126), column-major.
+template <typename T>
+int run_matrix(AnyCircuit* ac, void* data) {
+  auto* c = static_cast<qclab::QCircuit<T>*>(ac->c.get());
+  const auto M = c->matrix();
+  T* d = static_cast<T*>(data);
+  for (int64_t j = 0; j < M.cols(); ++j)
+    for (int64_t i = 0; i < M.rows(); ++i) d[i + j * M.rows()] = M(i, j);
+  return 0;
+}
+
+template <typename T>
+double run_nrmf(AnyCircuit* a, AnyCircuit* b) {
+  return qclab::nrmF(*static_cast<qclab::QCircuit<T>*>(a->c.get()),
+                     *static_cast<qclab::QCircuit<T>*>(b->c.get()));
+}
+
 }  // namespace
 
 extern "C" {
@@ -292,6 +325,42 @@ int ref_circuit_apply(void* c, void* v, char op, int offset) {
     case QSV_F32: return run<float>(ac, av, op, offset);
   }
   return 1;
+}
+
+int ref_circuit_apply_side(void* c, char side, char op, int nbQubits, int offset, void* data) {
+  auto* ac = static_cast<AnyCircuit*>(c);
+  switch (ac->dtype) {
+    case QSV_C128: return run_side<std::complex<double>>(ac, side, op, nbQubits, offset, data);
+    case QSV_C64: return run_side<std::complex<float>>(ac, side, op, nbQubits, offset, data);
+    case QSV_F64: return run_side<double>(ac, side, op, nbQubits, offset, data);
+    case QSV_F32: return run_side<float>(ac, side, op, nbQubits, offset, data);
+  }
+  return 1;
+}
+
+int ref_circuit_matrix(void* c, void* data) {
+  auto* ac = static_cast<AnyCircuit*>(c);
+  switch (ac->dtype) {
+    case QSV_C128: return run_matrix<std::complex<double>>(ac, data);
+    case QSV_C64: return run_matrix<std::complex<float>>(ac, data);
+    case QSV_F64: return run_matrix<double>(ac, data);
+    case QSV_F32: return run_matrix<float>(ac, data);
+  }
+  return 1;
+}
+
+// qclab::nrmF(circuit1, circuit2) (include/qclab/QCircuit.hpp:407-430).
+double ref_nrmF(void* a, void* b) {
+  auto* x = static_cast<AnyCircuit*>(a);
+  auto* y = static_cast<AnyCircuit*>(b);
+  if (x->dtype != y->dtype) return -1.0;
+  switch (x->dtype) {
+    case QSV_C128: return run_nrmf<std::complex<double>>(x, y);
+    case QSV_C64: return run_nrmf<std::complex<float>>(x, y);
+    case QSV_F64: return run_nrmf<double>(x, y);
+    case QSV_F32: return run_nrmf<float>(x, y);
+  }
+  return -1.0;
 }
 
 }  // extern "C"

@@ -53,6 +53,12 @@ class FuseOpts(C.Structure):
                 ("max_stage_gates", C.c_int), ("profile", C.c_int), ("reserved", C.c_int * 3)]
 
 
+class BatchOpts(C.Structure):
+    """``qsv_batch_opts``."""
+    _fields_ = [("tile_bits", C.c_int), ("low_bits", C.c_int), ("ctas_per_sm", C.c_int),
+                ("reserved", C.c_int * 5)]
+
+
 GATE_DTYPE = np.dtype([
     ("kind", np.int32), ("qubit0", np.int32), ("qubit1", np.int32),
     ("control_state", np.int32), ("cos", np.float64), ("sin", np.float64),
@@ -103,9 +109,18 @@ def _declare(lib):
         "qsv_apply_observable": ([p, p, C.c_char_p, C.POINTER(d), sz], i),
         "qsv_expectation_noalloc": ([p, i, i, p, C.c_char_p, C.POINTER(d), sz, C.POINTER(d)], i),
         "qsv_compare": ([p, p, C.POINTER(d)], i),
+        "qsv_normalize": ([p, C.POINTER(d)], i),
         "qsv_parse_qasm": ([C.c_char_p, i, p, sz, C.POINTER(sz), C.POINTER(i)], i),
         "qsv_adjoint_gradient": ([p, gp, sz, C.c_char_p, C.POINTER(d), sz, C.POINTER(d), i,
                                   C.POINTER(d)], i),
+        "qsv_batch_create": ([i, i, p, gp, p, C.c_char_p, p, p, p, p, C.POINTER(p)], i),
+        "qsv_batch_run": ([p, p, i], i),
+        "qsv_batch_results": ([p, p, p, p], i),
+        "qsv_batch_info": ([p, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(sz)], i),
+        "qsv_batch_destroy": ([p], i),
+        "qsv_set_identity": ([p], i),
+        "qsv_apply_matrix": ([p, gp, sz, C.c_char, C.c_char, i, i], i),
+        "qsv_nrmF": ([p, p, C.POINTER(d)], i),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)

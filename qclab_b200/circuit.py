@@ -13,7 +13,7 @@ import numpy as np
 from . import _lib as L
 from .gates import PARAMETRIC_KINDS, QObject
 from .state import StateVector, apply_records, to_records
-from .util import Op, as_op
+from .util import Op, Side, as_op
 
 
 class QCircuit(QObject):
@@ -119,12 +119,25 @@ class QCircuit(QObject):
                    if getattr(g, "KIND", None) in PARAMETRIC_KINDS and not g.fixed())
 
     # -- simulation ------------------------------------------------------------
-    def apply(self, op, nbQubits: int, vector, offset: int = 0, fused: bool = False):
-        """QCircuit::apply(op, nbQubits, vector, offset) (QCircuit.hpp:130-143)."""
+    def apply(self, op, nbQubits: int, vector, offset: int = 0, fused: bool = False, *rest):
+        """QCircuit::apply(op, nbQubits, vector, offset) (QCircuit.hpp:130-143):
+        every gate gets offset_ + offset (``records`` adds offset_).
+
+        With a Side first -- apply(side, op, nbQubits, matrix, offset) -- the
+        unitary update of QCircuit.hpp:176-204 on a host 2^n x 2^n array (in
+        place) or a device matrix object (see ``unitary``)."""
+        if isinstance(op, Side) or (isinstance(op, str) and op in ("L", "R")):
+            return self._apply_side(op, nbQubits, vector, offset, fused, *rest)
         dtype = vector.numpy_dtype if isinstance(vector, StateVector) else vector.dtype
-        recs = self.records(dtype, self._offset)
+        recs = self.records(dtype)
         apply_records(recs, as_op(op), nbQubits, vector, offset, fused)
         return vector
+
+    def matrix(self, dtype=np.complex128, fused: bool = False) -> np.ndarray:
+        """QCircuit::matrix() (QCircuit.hpp:120-126): the circuit's 2^n x 2^n
+        unitary, built on the GPU (eye, then every gate on the right)."""
+        from . import unitary as U
+        return U.circuit_matrix(self, dtype, fused)
 
     def simulate(self, vector, fused: bool = False):
         """QCircuit::simulate(vector) (QCircuit.hpp:164-166): in place."""

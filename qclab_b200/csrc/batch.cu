@@ -1,0 +1,702 @@
+// Batched variational sweep: many small circuits (each with its own qubit
+// count, gate list and Pauli-sum observable) -> energy <psi|H|psi> and the
+// full adjoint gradient of every circuit, in ONE persistent kernel launch
+// captured in a CUDA graph.
+//
+// Every CTA pulls circuit indices from an atomic work counter (largest
+// circuits first) and runs a whole circuit by itself:
+//   forward fused stages on psi  ->  lambda = H psi and E = <psi|lambda>
+//   ->  backward fused stages on (psi, lambda) with in-tile gradient terms.
+// A circuit whose two vectors fit in the CTA's shared memory (n <= m) never
+// touches global memory except for its results; larger circuits stream
+// their tiles through a per-CTA slot of a global workspace.  The stage and
+// pass plans come from the same planner as the single-state fused path
+// (stage_exec.cuh), packed for all circuits into one device buffer.
+// Gradient terms are summed tile by tile by the owning CTA in a fixed order,
+// so results are deterministic.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+#include "fused.hpp"
+#include "stage_exec.cuh"
+
+using namespace qsv;
+using namespace qsv::fx;
+
+struct qsv_batch_s {
+  qsv_dtype dtype = QSV_C64;
+  int ncirc = 0;
+  int tile_bits = 12;
+  int blocks = 0;
+  int threads = 256;
+  size_t smem = 0;
+  void* plan = nullptr;       // packed plan (device)
+  size_t plan_bytes = 0;
+  void* work = nullptr;       // per-CTA workspace (device)
+  size_t work_bytes = 0;
+  double* results = nullptr;  // [ncirc energies][grads] (device)
+  size_t nresults = 0;
+  unsigned* counter = nullptr;
+  std::vector<size_t> grad_off;  // per circuit, into the gradient part
+  std::vector<int> nparams;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t captured_on = nullptr;
+  // offsets of the plan sections
+  size_t off_jobs = 0, off_stages = 0, off_passes = 0, off_ops = 0, off_coefs = 0,
+         off_runoff = 0, off_groups = 0, off_terms = 0;
+};
+
+namespace {
+
+struct BStage {          // one fused stage of one circuit
+  int8_t bits[32];       // local tile bit -> global bit
+  int32_t m, full;
+  int32_t pass0, npasses, op0, coef0;  // into the plan arrays (absolute)
+  int32_t run0;                        // runoff offset (absolute)
+};
+
+struct BGroup {          // observable term group (terms whose flips fit a tile)
+  int8_t bits[32];
+  int32_t m;
+  int32_t term0, nterms;
+  int32_t run0;
+};
+
+struct BTerm {
+  uint32_t flip_local;
+  uint32_t pad;
+  uint64_t flip, zy;     // global masks
+  double wr, wi;         // coef * i^ny
+};
+
+struct BJob {
+  int32_t n, m, low;
+  int32_t fwd0, nfwd, bwd0, nbwd;   // stage ranges
+  int32_t grp0, ngrp;               // term-group range
+  int32_t circ;                     // circuit index (results)
+  int64_t grad_off;                 // into results (after the energies)
+};
+
+struct BArgs {
+  const BJob* jobs;
+  int njobs;
+  const BStage* stages;
+  const PassDev* passes;
+  const POp* ops;
+  const void* coefs;
+  const uint64_t* runoff;
+  const BGroup* groups;
+  const BTerm* terms;
+  void* work;
+  size_t work_stride;    // elements per CTA slot (2 vectors)
+  double* results;       // [ncirc] energies, then gradients
+  unsigned* counter;
+  int vec16;
+};
+
+// register passes with a block larger than the pass's thread groups
+// (threads >= 2^(m-R) idle in the pass but join every barrier/reduction)
+template <typename V, int NV, int R, bool FULL>
+__device__ __noinline__ void passes_b(V* t0, V* t1, const BStage& S, const BArgs& a, double2* red,
+                         double* grads) {
+  const PassDev* passes = a.passes + S.pass0;
+  const POp* ops = a.ops + S.op0;
+  const V* coefs = static_cast<const V*>(a.coefs) + S.coef0;
+  const uint32_t groups = 1u << (S.m - R);
+  const bool act = threadIdx.x < groups;
+  for (int pi = 0; pi < S.npasses; ++pi) {
+    const PassDev& P = passes[pi];
+    uint32_t tb = act ? threadIdx.x : 0;
+#pragma unroll
+    for (int k = 0; k < R; ++k) tb = ins0(tb, P.pos[k]);
+    const uint32_t ptb = phys<V>(tb);
+    V x[1 << R], y[1 << R];
+    if (act) {
+#pragma unroll
+      for (int j = 0; j < (1 << R); ++j) {
+        const uint32_t o = ptb ^ P.off[j];
+        x[j] = t0[o];
+        if (NV == 2) y[j] = t1[o];
+      }
+    }
+    for (int o = 0; o < P.nops; ++o) {
+      const POp op = ops[P.op0 + o];
+      if (op.shape == P_RED) {
+        if constexpr (NV == 2 && FULL) {
+          double im = 0.0;
+          if (act) {
+            const double2 s = red_dispatch<V, R>(x, y, op);
+            switch (op.ny & 3) {
+              case 0: im = s.y; break;
+              case 1: im = s.x; break;
+              case 2: im = -s.y; break;
+              default: im = -s.x; break;
+            }
+          }
+          const double2 tot = block_sum(make_double2(op.w * im, 0.0), red);
+          if (threadIdx.x == 0) grads[op.slot] += tot.x;
+        }
+      } else if (act) {
+        apply_reg<V, R, FULL>(x, op, coefs);
+        if (NV == 2) apply_reg<V, R, FULL>(y, op, coefs);
+      }
+    }
+    if (act) {
+#pragma unroll
+      for (int j = 0; j < (1 << R); ++j) {
+        const uint32_t o = ptb ^ P.off[j];
+        t0[o] = x[j];
+        if (NV == 2) t1[o] = y[j];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename V>
+__device__ __forceinline__ TileArgs stage_tile(const BStage& S, int n, int low,
+                                               const uint64_t* runoff) {
+  TileArgs ta;
+  ta.n = n;
+  ta.m = S.m;
+  ta.low = low;
+  for (int j = 0; j < 32; ++j) ta.bits[j] = S.bits[j];
+  ta.runoff = runoff + S.run0;
+  return ta;
+}
+
+// lambda (+)= H_group psi on a resident tile; returns this thread's
+// contribution to <psi|H_group psi>.
+template <typename V>
+__device__ __forceinline__ double apply_group(const V* t0, V* t1, const BGroup& G,
+                                              const BTerm* __restrict__ terms, uint64_t base,
+                                              const uint64_t* runoff, int low, bool accumulate) {
+  const uint32_t size = 1u << G.m, lowmask = (1u << low) - 1u;
+  double e = 0.0;
+  for (uint32_t el = threadIdx.x; el < size; el += blockDim.x) {
+    const uint64_t g = base | runoff[el >> low] | (el & lowmask);
+    double2 acc = accumulate ? to_d2(t1[phys<V>(el)]) : make_double2(0.0, 0.0);
+    double2 add = make_double2(0.0, 0.0);
+    for (int t = 0; t < G.nterms; ++t) {
+      const BTerm T = terms[G.term0 + t];
+      const double2 y = to_d2(t0[phys<V>(el ^ T.flip_local)]);
+      const double sg = (__popcll((g ^ T.flip) & T.zy) & 1) ? -1.0 : 1.0;
+      add.x = fma(sg * T.wr, y.x, fma(-sg * T.wi, y.y, add.x));
+      add.y = fma(sg * T.wr, y.y, fma(sg * T.wi, y.x, add.y));
+    }
+    const double2 x = to_d2(t0[phys<V>(el)]);
+    e += x.x * add.x + x.y * add.y;  // Re(conj(psi) * (H_g psi))
+    acc.x += add.x;
+    acc.y += add.y;
+    t1[phys<V>(el)] = from_d2<V>(acc);
+  }
+  return e;
+}
+
+template <typename V, int RF, int RB>
+__global__ void __launch_bounds__(256, 2)
+k_batch(BArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double2 red[32];
+  __shared__ int job_s;
+  V* t0 = reinterpret_cast<V*>(smem_raw);
+  for (;;) {
+    if (threadIdx.x == 0) job_s = (int)atomicAdd(a.counter, 1u);
+    __syncthreads();
+    const int jb = job_s;
+    __syncthreads();
+    if (jb >= a.njobs) break;
+    const BJob J = a.jobs[jb];
+    const uint32_t tsize = 1u << J.m;
+    V* t1 = t0 + tsize;
+    double* grads = a.results + J.grad_off;
+    const bool single = (J.m == J.n);
+    V* psi = static_cast<V*>(a.work) + (size_t)blockIdx.x * a.work_stride;
+    V* lam = psi + ((size_t)1 << J.n);
+    const uint64_t N = 1ull << J.n;
+    // (gradient accumulators were zeroed with the results before the launch)
+
+    // ---- psi = |0...0> ----
+    if (single) {
+      for (uint32_t e = threadIdx.x; e < tsize; e += blockDim.x)
+        t0[phys<V>(e)] = from_d2<V>(make_double2(e == 0 ? 1.0 : 0.0, 0.0));
+    } else {
+      for (uint64_t e = threadIdx.x; e < N; e += blockDim.x)
+        psi[e] = from_d2<V>(make_double2(e == 0 ? 1.0 : 0.0, 0.0));
+    }
+    __syncthreads();
+
+    // ---- forward ----
+    for (int s = 0; s < J.nfwd; ++s) {
+      const BStage S = a.stages[J.fwd0 + s];
+      if (single) {
+        if (S.full) passes_b<V, 1, RF, true>(t0, t1, S, a, red, grads);
+        else passes_b<V, 1, RF, false>(t0, t1, S, a, red, grads);
+      } else {
+        const TileArgs ta = stage_tile<V>(S, J.n, J.low, a.runoff);
+        const uint64_t ntiles = 1ull << (J.n - S.m);
+        for (uint64_t t = 0; t < ntiles; ++t) {
+          const uint64_t base = tile_base(ta, t);
+          load_tile<V, 1>(psi, nullptr, t0, nullptr, ta, base, a.vec16);
+          __syncthreads();
+          if (S.full) passes_b<V, 1, RF, true>(t0, t1, S, a, red, grads);
+          else passes_b<V, 1, RF, false>(t0, t1, S, a, red, grads);
+          store_tile<V, 1>(psi, nullptr, t0, nullptr, ta, base, a.vec16);
+          __syncthreads();
+        }
+      }
+    }
+
+    // ---- lambda = H psi, E = <psi|H|psi> ----
+    double e = 0.0;
+    if (J.ngrp == 0) {  // H = 0: lambda = 0
+      if (single) {
+        for (uint32_t el = threadIdx.x; el < tsize; el += blockDim.x) t1[el] = from_d2<V>(make_double2(0.0, 0.0));
+      } else {
+        for (uint64_t el = threadIdx.x; el < N; el += blockDim.x) lam[el] = from_d2<V>(make_double2(0.0, 0.0));
+      }
+      __syncthreads();
+    }
+    for (int g = 0; g < J.ngrp; ++g) {
+      const BGroup G = a.groups[J.grp0 + g];
+      if (single) {
+        e += apply_group<V>(t0, t1, G, a.terms, 0, a.runoff + G.run0, J.low, g > 0);
+        __syncthreads();
+      } else {
+        TileArgs ta;
+        ta.n = J.n;
+        ta.m = G.m;
+        ta.low = J.low;
+        for (int j = 0; j < 32; ++j) ta.bits[j] = G.bits[j];
+        ta.runoff = a.runoff + G.run0;
+        const uint64_t ntiles = 1ull << (J.n - G.m);
+        for (uint64_t t = 0; t < ntiles; ++t) {
+          const uint64_t base = tile_base(ta, t);
+          if (g > 0) load_tile<V, 2>(psi, lam, t0, t1, ta, base, a.vec16);
+          else load_tile<V, 1>(psi, nullptr, t0, nullptr, ta, base, a.vec16);
+          __syncthreads();
+          e += apply_group<V>(t0, t1, G, a.terms, base, ta.runoff, J.low, g > 0);
+          __syncthreads();
+          store_tile<V, 1>(lam, nullptr, t1, nullptr, ta, base, a.vec16);
+          __syncthreads();
+        }
+      }
+    }
+    const double2 et = block_sum(make_double2(e, 0.0), red);
+    if (threadIdx.x == 0) a.results[J.circ] = et.x;
+    __syncthreads();
+
+    // ---- backward: uncompute psi and lambda, gradient terms in-tile ----
+    for (int s = 0; s < J.nbwd; ++s) {
+      const BStage S = a.stages[J.bwd0 + s];
+      if (single) {
+        if (S.full) passes_b<V, 2, RB, true>(t0, t1, S, a, red, grads);
+        else passes_b<V, 2, RB, false>(t0, t1, S, a, red, grads);
+      } else {
+        const TileArgs ta = stage_tile<V>(S, J.n, J.low, a.runoff);
+        const uint64_t ntiles = 1ull << (J.n - S.m);
+        for (uint64_t t = 0; t < ntiles; ++t) {
+          const uint64_t base = tile_base(ta, t);
+          load_tile<V, 2>(psi, lam, t0, t1, ta, base, a.vec16);
+          __syncthreads();
+          if (S.full) passes_b<V, 2, RB, true>(t0, t1, S, a, red, grads);
+          else passes_b<V, 2, RB, false>(t0, t1, S, a, red, grads);
+          store_tile<V, 2>(psi, lam, t0, t1, ta, base, a.vec16);
+          __syncthreads();
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <typename V>
+constexpr int fwd_bits() { return reg_bits<V>(1); }
+template <typename V>
+constexpr int bwd_bits() { return reg_bits<V>(2); }
+
+struct HTermH {
+  uint64_t flip, zy;
+  int ny;
+  double coef;
+};
+
+qsv_status parse_obs(int n, const char* paulis, const double* coefs, size_t nt,
+                     std::vector<HTermH>* out) {
+  out->clear();
+  for (size_t t = 0; t < nt; ++t) {
+    HTermH h{0, 0, 0, coefs[t]};
+    for (int q = 0; q < n; ++q) {
+      const char c = paulis[t * (size_t)n + q];
+      const uint64_t b = 1ull << (n - 1 - q);
+      switch (c) {
+        case 'I': case 'i': break;
+        case 'X': case 'x': h.flip |= b; break;
+        case 'Y': case 'y': h.flip |= b; h.zy |= b; ++h.ny; break;
+        case 'Z': case 'z': h.zy |= b; break;
+        default: return fail(QSV_ERROR_INVALID_VALUE, "term %zu: '%c' is not I, X, Y or Z", t, c);
+      }
+    }
+    out->push_back(h);
+  }
+  return QSV_SUCCESS;
+}
+
+template <typename V>
+qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate* gates,
+                       const size_t* gate_off, const char* paulis, const size_t* char_off,
+                       const double* coefs, const size_t* term_off, const int* nparams,
+                       const qsv_batch_opts* opts) {
+  constexpr int RF = fwd_bits<V>(), RB = bwd_bits<V>();
+  const int M = (opts && opts->tile_bits > 0) ? opts->tile_bits : (sizeof(V) >= 16 ? 11 : 12);
+  const int low = (opts && opts->low_bits > 0) ? opts->low_bits : default_low_bits(sizeof(V));
+  if (M < RF || M - RB > 8 || M > 14)
+    return fail(QSV_ERROR_INVALID_VALUE, "batch tile_bits %d outside [%d, %d]", M, RF, RB + 8);
+  const size_t smem = (size_t(2) << M) * sizeof(V);
+  if (smem > 200 * 1024) return fail(QSV_ERROR_SIZE, "batch tiles exceed shared memory");
+
+  PackedPlan<V> plan;
+  std::vector<BStage> stages;
+  std::vector<BGroup> groups;
+  std::vector<BTerm> terms;
+  std::vector<BJob> jobs;
+  b->grad_off.assign(ncirc, 0);
+  b->nparams.assign(ncirc, 0);
+  size_t goff = ncirc;  // gradients follow the energies
+  int nmax = 0;
+  for (int c = 0; c < ncirc; ++c) {
+    const int n = nq[c];
+    if (n < RF || n > 30) return fail(QSV_ERROR_SIZE, "circuit %d: %d qubits outside [%d, 30]", c, n, RF);
+    nmax = std::max(nmax, n);
+    const int m = std::min(n, M);
+    const int lo = std::min(low, m);
+    const qsv_gate* g = gates + gate_off[c];
+    const size_t ng = gate_off[c + 1] - gate_off[c];
+    // forward
+    qsv_state_s fake;
+    fake.n = n;
+    fake.dtype = b->dtype;
+    std::vector<Lowered> fwd;
+    if (qsv_status st = lower_for_state(&fake, g, ng, 'N', 0, &fwd))
+      return fail(st, "circuit %d: %s", c, qsv_last_error());
+    // backward: [RED(param)] U^+ in reverse order
+    std::vector<Lowered> bwd;
+    for (size_t i = 0; i < ng; ++i) {
+      const size_t k = ng - 1 - i;
+      if (g[k].param >= 0) {
+        if (g[k].param >= nparams[c])
+          return fail(QSV_ERROR_INVALID_VALUE, "circuit %d gate %zu: param %d >= %d", c, k,
+                      g[k].param, nparams[c]);
+        Lowered R;
+        R.shape = SH_RED;
+        if (!generator_of(g[k], 0, n, &R.gen))
+          return fail(QSV_ERROR_NOT_SUPPORTED, "circuit %d gate %zu has no trainable angle", c, k);
+        R.slot = g[k].param;
+        bwd.push_back(R);
+      }
+      Lowered inv;
+      qsv_status st = dtype_double(b->dtype)
+          ? lower_gate<double>(g[k], 'C', 0, n, dtype_real(b->dtype), &inv)
+          : lower_gate<float>(g[k], 'C', 0, n, dtype_real(b->dtype), &inv);
+      if (st) return fail(st, "circuit %d gate %zu could not be inverted", c, k);
+      if (inv.shape != SH_NONE) bwd.push_back(inv);
+    }
+    BJob J{};
+    J.n = n;
+    J.m = m;
+    J.low = lo;
+    J.circ = c;
+    J.grad_off = (int64_t)goff;
+    b->grad_off[c] = goff - ncirc;
+    b->nparams[c] = nparams[c];
+    goff += nparams[c];
+    auto pack = [&](const std::vector<Lowered>& items, int r, int32_t* first, int32_t* count) {
+      const size_t s0 = plan.stages.size();
+      if (qsv_status st = pack_plan<V>(items, n, m, lo, r, 256, &plan)) return st;
+      *first = (int32_t)stages.size();
+      for (size_t si = s0; si < plan.stages.size(); ++si) {
+        const PackedStage& ps = plan.stages[si];
+        BStage S{};
+        for (int j = 0; j < 32; ++j) S.bits[j] = (int8_t)(j < ps.m ? ps.bits[j] : 0);
+        S.m = ps.m;
+        S.full = ps.full;
+        S.pass0 = (int32_t)ps.pass0;
+        S.npasses = (int32_t)ps.npasses;
+        S.op0 = (int32_t)ps.op0;
+        S.coef0 = (int32_t)ps.coef0;
+        S.run0 = (int32_t)ps.run0;
+        stages.push_back(S);
+      }
+      *count = (int32_t)(stages.size() - *first);
+      return QSV_SUCCESS;
+    };
+    if (qsv_status st = pack(fwd, RF, &J.fwd0, &J.nfwd)) return st;
+    if (qsv_status st = pack(bwd, RB, &J.bwd0, &J.nbwd)) return st;
+    // observable term groups (flip bits within an m-bit tile)
+    std::vector<HTermH> H;
+    const size_t nt = term_off[c + 1] - term_off[c];
+    if (qsv_status st = parse_obs(n, paulis ? paulis + char_off[c] : nullptr, coefs + term_off[c],
+                                  nt, &H))
+      return st;
+    const uint64_t lowmask = (1ull << lo) - 1ull;
+    std::vector<uint64_t> sets;
+    std::vector<std::vector<int>> members;
+    for (int t = 0; t < (int)H.size(); ++t) {
+      if (__builtin_popcountll(lowmask | H[t].flip) > m)
+        return fail(QSV_ERROR_NOT_SUPPORTED, "circuit %d term %d flips more than %d bits", c, t, m);
+      bool placed = false;
+      for (size_t k = 0; k < sets.size() && !placed; ++k)
+        if (__builtin_popcountll(sets[k] | H[t].flip) <= m) {
+          sets[k] |= H[t].flip;
+          members[k].push_back(t);
+          placed = true;
+        }
+      if (!placed) {
+        sets.push_back(lowmask | H[t].flip);
+        members.push_back({t});
+      }
+    }
+    J.grp0 = (int32_t)groups.size();
+    J.ngrp = (int32_t)sets.size();
+    for (size_t k = 0; k < sets.size(); ++k) {
+      BGroup G{};
+      int bits[64];
+      G.m = tile_bits_of(sets[k], n, m, bits);
+      for (int j = 0; j < 32; ++j) G.bits[j] = (int8_t)(j < G.m ? bits[j] : 0);
+      G.run0 = (int32_t)plan.runoff.size();
+      tile_runoffs(bits, G.m, lo, &plan.runoff);
+      int local_of[64];
+      for (int j = 0; j < 64; ++j) local_of[j] = -1;
+      for (int j = 0; j < G.m; ++j) local_of[bits[j]] = j;
+      G.term0 = (int32_t)terms.size();
+      G.nterms = (int32_t)members[k].size();
+      static const double pr[4] = {1, 0, -1, 0}, pi[4] = {0, 1, 0, -1};
+      for (int t : members[k]) {
+        BTerm T{};
+        for (int q = 0; q < n; ++q)
+          if ((H[t].flip >> q) & 1ull) T.flip_local |= 1u << local_of[q];
+        T.flip = H[t].flip;
+        T.zy = H[t].zy;
+        T.wr = H[t].coef * pr[H[t].ny & 3];
+        T.wi = H[t].coef * pi[H[t].ny & 3];
+        terms.push_back(T);
+      }
+      groups.push_back(G);
+    }
+    jobs.push_back(J);
+  }
+  // largest circuits first (static cost estimate: amplitudes x stages)
+  std::stable_sort(jobs.begin(), jobs.end(), [](const BJob& x, const BJob& y) {
+    return ((double)(1ull << x.n) * (x.nfwd + x.nbwd + 1)) > ((double)(1ull << y.n) * (y.nfwd + y.nbwd + 1));
+  });
+
+  auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
+  size_t off = 0;
+  b->off_jobs = off;   off = align(off + jobs.size() * sizeof(BJob));
+  b->off_stages = off; off = align(off + stages.size() * sizeof(BStage));
+  b->off_passes = off; off = align(off + plan.passes.size() * sizeof(PassDev));
+  b->off_ops = off;    off = align(off + plan.ops.size() * sizeof(POp));
+  b->off_coefs = off;  off = align(off + plan.coefs.size() * sizeof(V));
+  b->off_runoff = off; off = align(off + plan.runoff.size() * sizeof(uint64_t));
+  b->off_groups = off; off = align(off + groups.size() * sizeof(BGroup));
+  b->off_terms = off;  off = align(off + terms.size() * sizeof(BTerm));
+  std::vector<unsigned char> host(off, 0);
+  auto put = [&](size_t o, const void* p, size_t bytes) { if (bytes) std::memcpy(host.data() + o, p, bytes); };
+  put(b->off_jobs, jobs.data(), jobs.size() * sizeof(BJob));
+  put(b->off_stages, stages.data(), stages.size() * sizeof(BStage));
+  put(b->off_passes, plan.passes.data(), plan.passes.size() * sizeof(PassDev));
+  put(b->off_ops, plan.ops.data(), plan.ops.size() * sizeof(POp));
+  put(b->off_coefs, plan.coefs.data(), plan.coefs.size() * sizeof(V));
+  put(b->off_runoff, plan.runoff.data(), plan.runoff.size() * sizeof(uint64_t));
+  put(b->off_groups, groups.data(), groups.size() * sizeof(BGroup));
+  put(b->off_terms, terms.data(), terms.size() * sizeof(BTerm));
+
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (qsv_status st = cuda_status(cudaFuncSetAttribute(k_batch<V, RF, RB>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)smem), "batch smem attribute"))
+    return st;
+  int per_sm = 0;
+  const int threads = 1 << (M - RB) < 32 ? 32 : 1 << (M - RB);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<V, RF, RB>, threads, smem);
+  if (opts && opts->ctas_per_sm > 0) per_sm = std::min(per_sm, opts->ctas_per_sm);
+  if (per_sm < 1) return fail(QSV_ERROR_NOT_SUPPORTED, "batch kernel does not fit an SM");
+  b->blocks = std::min<int>(sms * per_sm, ncirc);
+  b->threads = threads;
+  b->smem = smem;
+  b->tile_bits = M;
+  const size_t stride = (size_t(2) << nmax);  // elements per CTA slot (psi + lambda)
+  if (nmax > M) {  // every CTA needs a slot: at most 8 GiB of workspace in all
+    const size_t cap = std::max<size_t>(1, (size_t(8) << 30) / (stride * sizeof(V)));
+    b->blocks = (int)std::min<size_t>((size_t)b->blocks, cap);
+  }
+  b->work_bytes = (nmax > M) ? (size_t)b->blocks * stride * sizeof(V) : 256;
+  b->nresults = goff;
+  b->plan_bytes = off;
+  if (qsv_status st = cuda_status(cudaMalloc(&b->plan, off), "batch plan")) return st;
+  if (qsv_status st = cuda_status(cudaMalloc(&b->work, b->work_bytes), "batch workspace")) return st;
+  if (qsv_status st = cuda_status(cudaMalloc(&b->results, goff * sizeof(double) + 256), "batch results"))
+    return st;
+  b->counter = reinterpret_cast<unsigned*>(reinterpret_cast<unsigned char*>(b->results) +
+                                           ((goff * sizeof(double) + 127) & ~size_t(127)));
+  return cuda_status(cudaMemcpy(b->plan, host.data(), off, cudaMemcpyHostToDevice), "batch plan upload");
+}
+
+template <typename V>
+qsv_status launch_batch(qsv_batch_s* b, cudaStream_t stream) {
+  constexpr int RF = fwd_bits<V>(), RB = bwd_bits<V>();
+  unsigned char* p = static_cast<unsigned char*>(b->plan);
+  BArgs a;
+  a.jobs = reinterpret_cast<const BJob*>(p + b->off_jobs);
+  a.njobs = b->ncirc;
+  a.stages = reinterpret_cast<const BStage*>(p + b->off_stages);
+  a.passes = reinterpret_cast<const PassDev*>(p + b->off_passes);
+  a.ops = reinterpret_cast<const POp*>(p + b->off_ops);
+  a.coefs = p + b->off_coefs;
+  a.runoff = reinterpret_cast<const uint64_t*>(p + b->off_runoff);
+  a.groups = reinterpret_cast<const BGroup*>(p + b->off_groups);
+  a.terms = reinterpret_cast<const BTerm*>(p + b->off_terms);
+  a.work = b->work;
+  a.work_stride = b->work_bytes > 256 ? b->work_bytes / sizeof(V) / b->blocks : 0;
+  a.results = b->results;
+  a.counter = b->counter;
+  a.vec16 = 1;
+  // zero the results (gradients accumulate) and the work counter
+  if (qsv_status st = cuda_status(cudaMemsetAsync(b->results, 0, b->nresults * sizeof(double), stream),
+                                  "batch results reset"))
+    return st;
+  if (qsv_status st = cuda_status(cudaMemsetAsync(b->counter, 0, sizeof(unsigned), stream),
+                                  "batch counter reset"))
+    return st;
+  k_batch<V, RF, RB><<<b->blocks, b->threads, b->smem, stream>>>(a);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "batch kernel launch");
+}
+
+qsv_status launch_any(qsv_batch_s* b, cudaStream_t stream) {
+  switch (b->dtype) {
+    case QSV_C64: return launch_batch<float2>(b, stream);
+    case QSV_C128: return launch_batch<double2>(b, stream);
+    default: return fail(QSV_ERROR_DTYPE, "batched sweeps need a complex dtype");
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+qsv_status qsv_batch_create(qsv_dtype dtype, int nCircuits, const int* nbQubits,
+                            const qsv_gate* gates, const size_t* gate_offsets,
+                            const char* paulis, const double* coefs, const size_t* term_offsets,
+                            const int* nParams, const qsv_batch_opts* opts, qsv_batch* out) {
+  if (!out) return fail(QSV_ERROR_INVALID_VALUE, "null output handle");
+  *out = nullptr;
+  if (nCircuits < 1 || !nbQubits || !gates || !gate_offsets || !term_offsets || !nParams)
+    return fail(QSV_ERROR_INVALID_VALUE, "null or empty batch description");
+  if (dtype != QSV_C64 && dtype != QSV_C128)
+    return fail(QSV_ERROR_DTYPE, "batched sweeps need complex<float> or complex<double>");
+  // term strings: circuit c's terms are nbQubits[c] characters each, back
+  // to back, so circuit c starts at character char_off[c]
+  std::vector<size_t> char_off(nCircuits + 1, 0);
+  for (int c = 0; c < nCircuits; ++c)
+    char_off[c + 1] = char_off[c] + (term_offsets[c + 1] - term_offsets[c]) * (size_t)nbQubits[c];
+  if (char_off[nCircuits] && (!paulis || !coefs))
+    return fail(QSV_ERROR_INVALID_VALUE, "null observable");
+  auto* b = new qsv_batch_s();
+  b->dtype = dtype;
+  b->ncirc = nCircuits;
+  const qsv_status st = (dtype == QSV_C64)
+      ? build_batch<float2>(b, nCircuits, nbQubits, gates, gate_offsets, paulis, char_off.data(),
+                            coefs, term_offsets, nParams, opts)
+      : build_batch<double2>(b, nCircuits, nbQubits, gates, gate_offsets, paulis, char_off.data(),
+                             coefs, term_offsets, nParams, opts);
+  if (st) {
+    qsv_batch_destroy(b);
+    return st;
+  }
+  *out = b;
+  return QSV_SUCCESS;
+}
+
+qsv_status qsv_batch_run(qsv_batch b, void* cuda_stream, int use_graph) {
+  if (!b) return fail(QSV_ERROR_INVALID_VALUE, "null batch");
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  if (!use_graph) return launch_any(b, stream);
+  if (!b->exec || b->captured_on != stream) {
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    cudaStream_t cap = stream;
+    bool own = false;
+    if (cap == nullptr) {  // the legacy stream cannot be captured
+      if (qsv_status st = cuda_status(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking),
+                                      "capture stream"))
+        return st;
+      own = true;
+    }
+    if (qsv_status st = cuda_status(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal),
+                                    "batch graph capture"))
+      return st;
+    qsv_status lst = launch_any(b, cap);
+    cudaGraph_t g = nullptr;
+    qsv_status est = cuda_status(cudaStreamEndCapture(cap, &g), "batch graph end capture");
+    if (lst || est) {
+      if (g) cudaGraphDestroy(g);
+      if (own) cudaStreamDestroy(cap);
+      return lst ? lst : est;
+    }
+    b->graph = g;
+    if (qsv_status st = cuda_status(cudaGraphInstantiate(&b->exec, g, 0), "batch graph instantiate")) {
+      if (own) cudaStreamDestroy(cap);
+      return st;
+    }
+    if (own) cudaStreamDestroy(cap);
+    b->captured_on = stream;
+  }
+  count_launch();
+  return cuda_status(cudaGraphLaunch(b->exec, stream), "batch graph launch");
+}
+
+qsv_status qsv_batch_results(qsv_batch b, void* cuda_stream, double* energies, double* grads) {
+  if (!b) return fail(QSV_ERROR_INVALID_VALUE, "null batch");
+  cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+  std::vector<double> host(b->nresults);
+  if (qsv_status st = cuda_status(cudaMemcpyAsync(host.data(), b->results,
+                                                  b->nresults * sizeof(double),
+                                                  cudaMemcpyDeviceToHost, stream), "batch results copy"))
+    return st;
+  if (qsv_status st = cuda_status(cudaStreamSynchronize(stream), "batch results synchronize"))
+    return st;
+  if (energies) std::memcpy(energies, host.data(), b->ncirc * sizeof(double));
+  if (grads && b->nresults > (size_t)b->ncirc)
+    std::memcpy(grads, host.data() + b->ncirc, (b->nresults - b->ncirc) * sizeof(double));
+  return QSV_SUCCESS;
+}
+
+qsv_status qsv_batch_info(qsv_batch b, int* blocks, int* threads, int* tile_bits,
+                          size_t* workspace_bytes) {
+  if (!b) return fail(QSV_ERROR_INVALID_VALUE, "null batch");
+  if (blocks) *blocks = b->blocks;
+  if (threads) *threads = b->threads;
+  if (tile_bits) *tile_bits = b->tile_bits;
+  if (workspace_bytes) *workspace_bytes = b->work_bytes;
+  return QSV_SUCCESS;
+}
+
+qsv_status qsv_batch_destroy(qsv_batch b) {
+  if (!b) return QSV_SUCCESS;
+  cudaDeviceSynchronize();
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->plan) cudaFree(b->plan);
+  if (b->work) cudaFree(b->work);
+  if (b->results) cudaFree(b->results);
+  delete b;
+  return QSV_SUCCESS;
+}
+
+}  // extern "C"

@@ -62,6 +62,15 @@ k_inner(const V* __restrict__ a, const V* __restrict__ b, uint64_t N, double2* _
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
+// x *= s (s formed in FP64, applied in the element's precision)
+template <typename V>
+__global__ void __launch_bounds__(kRedThreads)
+k_scale_real(V* __restrict__ st, uint64_t N, double s) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < N;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    st[i] = from_d2<V>(make_double2(to_d2(st[i]).x * s, to_d2(st[i]).y * s));
+}
+
 // Fixed-order sum of `count` partials by one block.
 __global__ void __launch_bounds__(1024)
 k_final(const double2* __restrict__ partial, int count, double2* __restrict__ out) {
@@ -570,6 +579,24 @@ qsv_status qsv_norm2(qsv_state s, double* out) {
     case QSV_F32:  return norm2_typed<float>(s, out);
   }
   return fail(QSV_ERROR_INVALID_VALUE, "bad dtype");
+}
+
+qsv_status qsv_normalize(qsv_state s, double* norm2_out) {
+  double nrm = 0.0;
+  if (qsv_status st = qsv_norm2(s, &nrm)) return st;
+  if (norm2_out) *norm2_out = nrm;
+  if (!(nrm > 0.0)) return fail(QSV_ERROR_INVALID_VALUE, "cannot normalise a zero state");
+  const double inv = 1.0 / std::sqrt(nrm);
+  const uint64_t N = dim(s->n);
+  const unsigned blocks = (unsigned)std::min<uint64_t>(kRedBlocks, (N + kRedThreads - 1) / kRedThreads);
+  switch (s->dtype) {
+    case QSV_C128: k_scale_real<double2><<<blocks, kRedThreads, 0, s->stream>>>((double2*)s->d, N, inv); break;
+    case QSV_C64:  k_scale_real<float2><<<blocks, kRedThreads, 0, s->stream>>>((float2*)s->d, N, inv); break;
+    case QSV_F64:  k_scale_real<double><<<blocks, kRedThreads, 0, s->stream>>>((double*)s->d, N, inv); break;
+    case QSV_F32:  k_scale_real<float><<<blocks, kRedThreads, 0, s->stream>>>((float*)s->d, N, inv); break;
+  }
+  count_launch();
+  return cuda_status(cudaGetLastError(), "normalise launch");
 }
 
 qsv_status qsv_inner(qsv_state a, qsv_state b, double* out) {

@@ -23,7 +23,7 @@ import math
 import numpy as np
 
 from . import _lib as L
-from .util import Op, as_op
+from .util import Op, Side, as_op
 
 
 def _real_of(dtype) -> type:
@@ -70,17 +70,43 @@ class QObject:
         """Flat gate records of this object (with a qubit offset)."""
         raise NotImplementedError
 
-    def apply(self, op, nbQubits: int, vector, offset: int = 0, fused: bool = False):
+    def apply(self, op, nbQubits: int, vector, offset: int = 0, fused: bool = False, *rest):
         """Applies this object to ``vector`` in place, like
         ``QObject<T>::apply(op, nbQubits, vector, offset)`` (QObject.hpp:52-53).
         ``vector`` is a host numpy array (copied to the GPU and back) or a
-        device-resident :class:`StateVector`."""
+        device-resident :class:`StateVector`.
+
+        ``apply(side, op, nbQubits, matrix, offset=0, fused=False)`` (a Side
+        first, positional) is the unitary update ``QObject<T>::apply(Side,
+        Op, nbQubits, SquareMatrix<T>&, offset)``: side Right gives
+        matrix <- op(G) matrix, Left matrix <- matrix op(G)."""
+        if isinstance(op, Side) or (isinstance(op, str) and op in ("L", "R")):
+            return self._apply_side(op, nbQubits, vector, offset, fused, *rest)
         from .state import apply_records
         op = as_op(op)
         dtype = vector.dtype if not hasattr(vector, "numpy_dtype") else vector.numpy_dtype
         recs = self.records(dtype, 0)
         apply_records(recs, op, nbQubits, vector, offset, fused)
         return vector
+
+    def _apply_side(self, side, op, nbQubits: int, matrix, offset=0, fused=False):
+        """The Side form of ``apply`` on a host 2^n x 2^n numpy array (in
+        place) or a device matrix object of 2n qubits."""
+        from . import unitary as U
+        from .state import StateVector
+        offset = int(offset)
+        if isinstance(matrix, StateVector):
+            if matrix.nbQubits != 2 * nbQubits:
+                raise ValueError("matrix object does not hold a 2^nbQubits square matrix")
+            U.apply_side(matrix, self.records(matrix.numpy_dtype), side, op, offset, bool(fused))
+            return matrix
+        N = 1 << nbQubits
+        if not isinstance(matrix, np.ndarray) or matrix.shape != (N, N):
+            raise ValueError("matrix must be a 2^nbQubits x 2^nbQubits numpy array")
+        with U.upload(matrix) as m:
+            U.apply_side(m, self.records(matrix.dtype), side, op, offset, bool(fused))
+            matrix[...] = U.download(m)
+        return matrix
 
     def __repr__(self) -> str:
         return f"{type(self).__name__}({self.qubits()})"

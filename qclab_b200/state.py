@@ -198,6 +198,14 @@ def _compare(self, other: "StateVector"):
     return complex(out[0], out[1]), out[2]
 
 
+def _normalize(self) -> float:
+    """Scales the state to unit norm (norm in FP64); returns <psi|psi> before."""
+    out = C.c_double()
+    L.check(self._lib.qsv_normalize(self._h, C.byref(out)), "qsv_normalize")
+    return out.value
+
+
+StateVector.normalize = _normalize
 StateVector.compare = _compare
 StateVector.norm2 = _norm2
 StateVector.inner = _inner

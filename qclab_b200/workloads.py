@@ -80,9 +80,13 @@ def random_unitary(dim: int, rng) -> np.ndarray:
     return q * (np.diag(r) / np.abs(np.diag(r)))
 
 
-def random_mixed(n: int, count: int, seed: int = 0, real: bool = False) -> QCircuit:
+def random_mixed(n: int, count: int, seed: int = 0, real: bool = False,
+                 adjacent_generic: bool = False) -> QCircuit:
     """Random circuit over all gate classes (real-coefficient ones only for
-    ``real=True``)."""
+    ``real=True``).  ``adjacent_generic`` puts the generic 2-qubit gates
+    (RotationXX/YY/ZZ, MatrixGate2) on neighbouring qubits, the only
+    placement QCLAB++'s unitary update of such gates accepts
+    (src/qgates/QGate2.cpp:41)."""
     rng = np.random.default_rng(seed)
     c = QCircuit(n)
     one = [G.Identity, G.Hadamard, G.PauliX, G.PauliY, G.PauliZ, G.RotationX, G.RotationY,
@@ -112,6 +116,9 @@ def random_mixed(n: int, count: int, seed: int = 0, real: bool = False) -> QCirc
             t = two[int(rng.integers(0, len(two)))]
             th = float(rng.uniform(0, 2 * math.pi))
             cs = int(rng.integers(0, 2))
+            if adjacent_generic and t in (G.RotationXX, G.RotationYY, G.RotationZZ, "M2", "M2r"):
+                a = min(a, b, n - 2)
+                b = a + 1
             if t == "M2":
                 c.push_back(G.MatrixGate2(a, b, random_unitary(4, rng)))
             elif t == "M2r":

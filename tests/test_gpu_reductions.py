@@ -79,6 +79,24 @@ def test_apply_observable(cuda, dtype, n):
         assert np.max(np.abs(b.download() - ref)) <= tol * max(1.0, np.max(np.abs(ref)))
 
 
+def test_compare_mixed_precision_and_normalize(cuda):
+    n = 15
+    x = rand_state(n, np.complex128, 9)
+    with StateVector(n, np.complex64) as a, StateVector(n, np.complex128) as b:
+        xf = (1.01 * x).astype(np.complex64)
+        a.upload(xf)
+        b.upload(x)
+        ip, mx = a.compare(b)
+        ref_ip = np.vdot(xf.astype(np.complex128), x)
+        assert abs(ip - ref_ip) < 1e-12
+        assert abs(mx - np.max(np.abs(xf.astype(np.complex128) - x))) < 1e-15
+        before = a.normalize()
+        assert abs(before - np.vdot(xf.astype(np.complex128), xf.astype(np.complex128)).real) < 1e-12
+        assert abs(a.norm2() - 1.0) < 1e-6
+        y = a.download().astype(np.complex128)
+        assert np.max(np.abs(y - x)) < 1e-6
+
+
 def test_reduction_errors(cuda):
     with StateVector(3, np.float64) as a, StateVector(3, np.float64) as b:
         H = Observable(3).add(1.0, "XYZ")
