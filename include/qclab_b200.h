@@ -172,6 +172,12 @@ qsv_status qsv_plan_stats(int nbQubits, qsv_dtype dtype, const qsv_gate* gates,
                           size_t nGates, char op, int offset,
                           const qsv_fuse_opts* opts, int* nStages,
                           int* stage_gates, int capacity);
+/* Host only (new): totals of the same plan -- stages, register passes (one
+ * shared-memory round trip of a tile each) and ops. */
+qsv_status qsv_plan_passes(int nbQubits, qsv_dtype dtype, const qsv_gate* gates,
+                           size_t nGates, char op, int offset,
+                           const qsv_fuse_opts* opts, int* nStages, int* nPasses,
+                           int* nOps);
 
 /* ---- FP64 reductions (new: QCLAB++ has no observables) -------------------
  * All sums accumulate in double precision whatever the state's dtype, with

@@ -79,25 +79,39 @@ class UserGate1 : public qclab::qgates::QGate1<T> {
 // A user 2-qubit gate (generic QGate2::apply).  `m` is in the order the
 // reference's apply4 lambda uses (x1..x4 = |00>,|10>,|01>,|11> of the
 // sorted qubits).
+// The state path (apply4) pairs slots differently from the kron basis, so
+// the gate carries two matrices: `m` in apply4 slot order for the vector
+// apply, `k` in the kron basis of the sorted qubits for the unitary update
+// apply(Side, ...), whose loops use the kron order (src/qgates/QGate2.cpp:32-108).
 template <typename T>
 class UserGate2 : public qclab::qgates::QGate2<T> {
  public:
-  UserGate2(int q0, int q1, const T* m)
+  UserGate2(int q0, int q1, const T* m, const T* k)
       : q_{std::min(q0, q1), std::max(q0, q1)},
         mat_(m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7], m[8], m[9], m[10], m[11], m[12],
-             m[13], m[14], m[15]) {}
+             m[13], m[14], m[15]),
+        kron_(k[0], k[1], k[2], k[3], k[4], k[5], k[6], k[7], k[8], k[9], k[10], k[11], k[12],
+              k[13], k[14], k[15]) {}
   bool fixed() const override { return true; }
   bool controlled() const override { return false; }
   int qubit() const override { return q_[0]; }
   std::vector<int> qubits() const override { return {q_[0], q_[1]}; }
   void setQubits(const int* q) override { q_[0] = q[0]; q_[1] = q[1]; }
-  qclab::dense::SquareMatrix<T> matrix() const override { return mat_; }
+  qclab::dense::SquareMatrix<T> matrix() const override { return side_ ? kron_ : mat_; }
   int toQASM(std::ostream&, const int = 0) const override { return -1; }
+  using qclab::qgates::QGate2<T>::apply;
+  void apply(qclab::Side side, qclab::Op op, const int nbQubits,
+             qclab::dense::SquareMatrix<T>& matrix, const int offset = 0) const override {
+    side_ = true;
+    qclab::qgates::QGate2<T>::apply(side, op, nbQubits, matrix, offset);
+    side_ = false;
+  }
 
  protected:
   bool equals(const qclab::QObject<T>&) const override { return false; }
   int q_[2];
-  qclab::dense::SquareMatrix<T> mat_;
+  qclab::dense::SquareMatrix<T> mat_, kron_;
+  mutable bool side_ = false;
 };
 
 // A user controlled gate (generic QControlledGate2::apply).
@@ -151,7 +165,12 @@ int add_gate(qclab::QCircuit<T>& c, const qsv_gate& g) {
       }
       for (int r = 0; r < 4; ++r)
         for (int cc = 0; cc < 4; ++cc) m[r * 4 + cc] = entry<T>(g.matrix, 4, slot_of[r], slot_of[cc]);
-      p = std::make_unique<UserGate2<T>>(a, b, m);
+      // kron basis of the sorted qubits: index 2 bit(min) + bit(max)
+      T k[16];
+      auto kron_of = [&](int s) { return (a == q0) ? s : (((s & 1) << 1) | (s >> 1)); };
+      for (int r = 0; r < 4; ++r)
+        for (int cc = 0; cc < 4; ++cc) k[r * 4 + cc] = entry<T>(g.matrix, 4, kron_of(r), kron_of(cc));
+      p = std::make_unique<UserGate2<T>>(a, b, m, k);
       break;
     }
     default:

@@ -101,6 +101,8 @@ def _declare(lib):
         "qsv_apply": ([p, gp, sz, C.c_char, i], i),
         "qsv_apply_fused": ([p, gp, sz, C.c_char, i, p], i),
         "qsv_plan_stats": ([i, i, gp, sz, C.c_char, i, p, C.POINTER(i), p, i], i),
+        "qsv_plan_passes": ([i, i, gp, sz, C.c_char, i, p, C.POINTER(i), C.POINTER(i),
+                             C.POINTER(i)], i),
         "qsv_apply_host": ([i, i, p, gp, sz, C.c_char, i, i], i),
         "qsv_last_stage_times": ([C.POINTER(C.c_float), i, C.POINTER(i)], i),
         "qsv_norm2": ([p, C.POINTER(d)], i),

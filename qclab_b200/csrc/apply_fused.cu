@@ -41,11 +41,14 @@ template <typename V>
 qsv_status pack_plan(const std::vector<Lowered>& gates, int n, int m, int low, int r,
                      int max_gates, PackedPlan<V>* out) {
   constexpr bool cplx = Elem<V>::cplx;
-  std::vector<Stage> stages = plan_stages(gates, n, m, low, max_gates);
+  std::vector<Stage> stages =
+      plan_stages(gates, n, m, low, max_gates, kMaxRed, kPlanSmemMax, sizeof(V));
   for (const Stage& stg : stages) {
     PackedStage ps;
     ps.m = stg.m;
     ps.full = 0;
+    ps.red0 = out->red_slots.size();
+    ps.nred = 0;
     for (int gi : stg.gates)
       if (gates[gi].shape == SH_QUAD || gates[gi].shape == SH_RED) ps.full = 1;
     for (int j = 0; j < 64; ++j) ps.bits[j] = (j < stg.m) ? stg.bits[j] : 0;
@@ -140,6 +143,9 @@ qsv_status pack_plan(const std::vector<Lowered>& gates, int n, int m, int low, i
             op.ny = (int8_t)L.gen.ny;
             op.w = (int8_t)L.gen.w;
             op.slot = L.slot;
+            if (ps.nred >= kMaxRed) return fail(QSV_ERROR_INVALID_VALUE, "internal: stage reductions");
+            op.ridx = (int16_t)ps.nred++;
+            out->red_slots.push_back(L.slot);
             break;
           }
           default:
@@ -151,6 +157,10 @@ qsv_status pack_plan(const std::vector<Lowered>& gates, int n, int m, int low, i
       out->passes.push_back(pd);
     }
     ps.npasses = out->passes.size() - ps.pass0;
+    ps.nops = (int)(out->ops.size() - ps.op0);
+    ps.ncoef = (int)(out->coefs.size() - ps.coef0);
+    if (plan_smem_bytes<V>((int)ps.npasses, ps.nops, ps.ncoef) > kPlanSmemMax)
+      return fail(QSV_ERROR_INVALID_VALUE, "internal: stage plan exceeds its shared-memory budget");
     tile_runoffs(stg.bits, stg.m, low, &out->runoff);
     out->stages.push_back(ps);
   }
@@ -164,6 +174,12 @@ template qsv_status pack_plan<float>(const std::vector<Lowered>&, int, int, int,
 
 }  // namespace fx
 
+// Register bits of a pass for a tile of m bits (fewer for tiny tiles).
+int pass_bits(size_t eb, int nv, int m) {
+  const int rdef = (eb >= 16) ? fx::reg_bits<double2>(nv) : fx::reg_bits<float2>(nv);
+  return (m >= rdef) ? rdef : (m >= 2 ? 2 : 1);
+}
+
 namespace {
 
 using namespace fx;
@@ -174,31 +190,46 @@ struct Stage2Args {
   const PassDev* passes;
   const POp* ops;
   const void* coefs;
-  double* partial;  // [slot][tile] partial sums of the RED ops
-  int vec16;        // 16-byte cp.async copies allowed (alignment and run length)
-};
-
-struct PartialSink {
-  double* partial;
-  __device__ void operator()(int slot, double v) const {
-    partial[(size_t)slot * gridDim.x + blockIdx.x] = v;
-  }
+  double* partial;           // [slot][tile] partial sums of the RED ops
+  const int32_t* red_slots;  // slot of each of the stage's nred reductions
+  int nred;
+  int nops, ncoef;           // the stage's ops and coefficients (staged in shared memory)
+  int vec16;                 // 16-byte cp.async copies allowed (alignment and run length)
 };
 
 template <typename V, int NV, int R, bool FULL>
-__global__ void __launch_bounds__(256, min_blocks<V>())
+__global__ void __launch_bounds__(256, min_blocks<V, NV>())
 k_stage2(V* __restrict__ v0, V* __restrict__ v1, Stage2Args a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double2 red[32];
   const uint32_t size = 1u << a.ta.m;
   V* t0 = reinterpret_cast<V*>(smem_raw);
   V* t1 = t0 + size;
+  // gradient accumulators after the tiles (allocated for two-vector sweeps),
+  // then the stage's plan
+  double* racc = reinterpret_cast<double*>(smem_raw + size_t(NV) * size * sizeof(V));
+  unsigned char* plan = smem_raw + size_t(NV) * size * sizeof(V) + (NV == 2 ? kRaccBytes : 0);
+  const PassDev* passes;
+  const POp* ops;
+  const V* coefs;
+  stage_plan<V>(plan, a.passes, a.npasses, a.ops, a.nops, static_cast<const V*>(a.coefs),
+                a.ncoef, &passes, &ops, &coefs);
+  const bool red = NV == 2 && FULL && a.nred > 0;
+  if (red)
+    for (int i = threadIdx.x; i < a.nred * kRedWarps; i += blockDim.x) racc[i] = 0.0;
   const uint64_t base = tile_base(a.ta, blockIdx.x);
   load_tile<V, NV>(v0, v1, t0, t1, a.ta, base, a.vec16);
   __syncthreads();
-  run_passes<V, NV, R, FULL>(t0, t1, a.passes, a.npasses, a.ops, static_cast<const V*>(a.coefs),
-                             red, PartialSink{a.partial});
+  run_passes<V, NV, R, FULL, turn_bits<V>(NV)>(t0, t1, passes, a.npasses, ops, coefs, racc,
+                                                size >> R);
   store_tile<V, NV>(v0, v1, t0, t1, a.ta, base, a.vec16);
+  if (red) {  // run_passes ended with a barrier: racc is complete
+    const int warps = red_warps();
+    for (int r = threadIdx.x; r < a.nred; r += blockDim.x) {
+      double t = 0.0;
+      for (int w = 0; w < warps; ++w) t += racc[r * kRedWarps + w];
+      a.partial[(size_t)a.red_slots[r] * gridDim.x + blockIdx.x] = t;
+    }
+  }
 }
 
 // Fixed-order sum of each row of partial[rows][cols] (one block per row).
@@ -230,16 +261,13 @@ qsv_status execute_typed(const ExecArgs& x) {
   qsv_state_s* s = x.s;
   const int n = s->n;
   const qsv_fuse_opts* opts = x.opts;
-  int m = (opts && opts->tile_bits > 0) ? opts->tile_bits : default_tile_bits(sizeof(V), x.nv);
+  const int m = effective_tile_bits(sizeof(V), x.nv, n, opts);
   int low = (opts && opts->low_bits > 0) ? opts->low_bits : default_low_bits(sizeof(V));
   const int max_gates = (opts && opts->max_stage_gates > 0) ? opts->max_stage_gates : 256;
-  if (m > 14) m = 14;
-  if (m > n) m = n;
-  const int rdef = (x.nv == 2) ? reg_bits<V>(2) : reg_bits<V>(1);
-  const int r = (m >= rdef) ? rdef : (m >= 2 ? 2 : 1);
-  if (m - r > 8) m = r + 8;  // at most 256 threads per CTA
+  const int r = pass_bits(sizeof(V), x.nv, m);
   if (low > m) low = m;
-  const size_t smem = (size_t(1) << m) * sizeof(V) * x.nv;
+  const size_t smem_fixed = (size_t(1) << m) * sizeof(V) * x.nv + (x.nv == 2 ? kRaccBytes : 0);
+  const size_t smem = smem_fixed + kPlanSmemMax;  // bound; each launch asks for its own size
   if (smem > 200 * 1024)
     return fail(QSV_ERROR_SIZE, "tile of %d x 2^%d elements exceeds shared memory", x.nv, m);
   // 16-byte copies need 16-byte aligned vectors and runs of >= 16 bytes
@@ -257,12 +285,15 @@ qsv_status execute_typed(const ExecArgs& x) {
   const size_t op_off = align(pass_bytes);
   const size_t coef_off = align(op_off + plan.ops.size() * sizeof(POp));
   const size_t run_off = align(coef_off + plan.coefs.size() * sizeof(V));
-  const size_t total = run_off + plan.runoff.size() * sizeof(uint64_t);
+  const size_t red_off = align(run_off + plan.runoff.size() * sizeof(uint64_t));
+  const size_t total = red_off + plan.red_slots.size() * sizeof(int32_t);
   std::vector<unsigned char> host(total);
   std::memcpy(host.data(), plan.passes.data(), pass_bytes);
   std::memcpy(host.data() + op_off, plan.ops.data(), plan.ops.size() * sizeof(POp));
   std::memcpy(host.data() + coef_off, plan.coefs.data(), plan.coefs.size() * sizeof(V));
   std::memcpy(host.data() + run_off, plan.runoff.data(), plan.runoff.size() * sizeof(uint64_t));
+  if (!plan.red_slots.empty())
+    std::memcpy(host.data() + red_off, plan.red_slots.data(), plan.red_slots.size() * sizeof(int32_t));
   if (qsv_status st = ensure_scratch(s, total)) return st;
   unsigned char* dev = static_cast<unsigned char*>(s->scratch);
   if (qsv_status st = cuda_status(cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice,
@@ -276,7 +307,7 @@ qsv_status execute_typed(const ExecArgs& x) {
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024),
             "fused stage shared-memory attribute"))
       return st;
-  const unsigned threads = 1u << (m - r);
+  const unsigned threads = 1u << std::min(m - r, 8);
   const uint64_t ntiles = 1ull << (n - m);
   if (x.ntiles_out) *x.ntiles_out = ntiles;
   if (x.nslots > 0 && x.partial_bytes < (size_t)x.nslots * ntiles * sizeof(double))
@@ -304,11 +335,16 @@ qsv_status execute_typed(const ExecArgs& x) {
     a.ops = reinterpret_cast<const POp*>(dev + op_off) + ps.op0;
     a.coefs = dev + coef_off + ps.coef0 * sizeof(V);
     a.partial = x.partial;
+    a.red_slots = reinterpret_cast<const int32_t*>(dev + red_off) + ps.red0;
+    a.nred = ps.nred;
+    a.nops = ps.nops;
+    a.ncoef = ps.ncoef;
+    const size_t smem_stage = smem_fixed + plan_smem_bytes<V>((int)ps.npasses, ps.nops, ps.ncoef);
     a.vec16 = vec16 ? 1 : 0;
     void* args[] = {&p0, &p1, &a};
     if (qsv_status st = cuda_status(cudaLaunchKernel(kerns[ps.full ? 1 : 0], dim3((unsigned)ntiles),
                                                      dim3(threads),
-                                                     args, smem, s->stream),
+                                                     args, smem_stage, s->stream),
                                     "fused stage launch"))
       return st;
     count_launch();
@@ -336,6 +372,16 @@ qsv_status execute_typed(const ExecArgs& x) {
 }  // namespace
 
 int default_tile_bits(size_t eb, int nv) { return (eb >= 16 ? 12 : 13) - (nv == 2 ? 1 : 0); }
+
+int effective_tile_bits(size_t eb, int nv, int n, const qsv_fuse_opts* opts) {
+  int m = (opts && opts->tile_bits > 0) ? opts->tile_bits : default_tile_bits(eb, nv);
+  if (m > 14) m = 14;
+  if (m > n) m = n;
+  const int r = pass_bits(eb, nv, m);
+  const int turns = (eb >= 16) ? fx::turn_bits<double2>(nv) : fx::turn_bits<float2>(nv);
+  if (m - r > 8 + turns) m = r + 8 + turns;  // at most 256 threads per CTA
+  return m;
+}
 int default_low_bits(size_t eb) { return eb >= 16 ? 2 : 3; }
 
 qsv_status execute_fused(const ExecArgs& x) {
@@ -368,12 +414,29 @@ extern "C" qsv_status qsv_last_stage_times(float* ms, int capacity, int* count) 
   return QSV_SUCCESS;
 }
 
-extern "C" qsv_status qsv_plan_stats(int nbQubits, qsv_dtype dtype, const qsv_gate* gates,
-                                     size_t nGates, char op, int offset,
-                                     const qsv_fuse_opts* opts, int* nStages, int* stage_gates,
-                                     int capacity) {
-  using namespace qsv;
-  if (!nStages) return fail(QSV_ERROR_INVALID_VALUE, "null nStages");
+namespace qsv {
+namespace {
+
+// The executor's plan of a single-vector sweep: ops and passes per stage.
+template <typename V>
+qsv_status plan_counts(const std::vector<Lowered>& low, int n, const qsv_fuse_opts* opts,
+                       std::vector<int>* ops, std::vector<int>* passes) {
+  const int m = effective_tile_bits(sizeof(V), 1, n, opts);
+  const int lowb = (opts && opts->low_bits > 0) ? opts->low_bits : default_low_bits(sizeof(V));
+  const int max_gates = (opts && opts->max_stage_gates > 0) ? opts->max_stage_gates : 256;
+  fx::PackedPlan<V> plan;
+  if (qsv_status st = fx::pack_plan<V>(low, n, m, lowb, pass_bits(sizeof(V), 1, m), max_gates, &plan))
+    return st;
+  for (const fx::PackedStage& ps : plan.stages) {
+    ops->push_back(ps.nops);
+    passes->push_back((int)ps.npasses);
+  }
+  return QSV_SUCCESS;
+}
+
+qsv_status plan_counts_any(int nbQubits, qsv_dtype dtype, const qsv_gate* gates, size_t nGates,
+                           char op, int offset, const qsv_fuse_opts* opts, std::vector<int>* ops,
+                           std::vector<int>* passes) {
   if (!dtype_valid(dtype)) return fail(QSV_ERROR_INVALID_VALUE, "bad dtype");
   if (nbQubits < 1 || nbQubits > kMaxQubits) return fail(QSV_ERROR_SIZE, "bad nbQubits");
   qsv_state_s fake;
@@ -381,14 +444,47 @@ extern "C" qsv_status qsv_plan_stats(int nbQubits, qsv_dtype dtype, const qsv_ga
   fake.dtype = dtype;
   std::vector<Lowered> low;
   if (qsv_status st = lower_for_state(&fake, gates, nGates, op, offset, &low)) return st;
-  const size_t eb = elem_bytes(dtype);
-  int m = (opts && opts->tile_bits > 0) ? opts->tile_bits : default_tile_bits(eb, 1);
-  int lowb = (opts && opts->low_bits > 0) ? opts->low_bits : default_low_bits(eb);
-  const int max_gates = (opts && opts->max_stage_gates > 0) ? opts->max_stage_gates : 256;
-  std::vector<Stage> stages = plan_stages(low, nbQubits, std::min(m, 14), lowb, max_gates);
-  *nStages = (int)stages.size();
+  switch (dtype) {
+    case QSV_C128: return plan_counts<double2>(low, nbQubits, opts, ops, passes);
+    case QSV_C64:  return plan_counts<float2>(low, nbQubits, opts, ops, passes);
+    case QSV_F64:  return plan_counts<double>(low, nbQubits, opts, ops, passes);
+    default:       return plan_counts<float>(low, nbQubits, opts, ops, passes);
+  }
+}
+
+}  // namespace
+}  // namespace qsv
+
+extern "C" qsv_status qsv_plan_stats(int nbQubits, qsv_dtype dtype, const qsv_gate* gates,
+                                     size_t nGates, char op, int offset,
+                                     const qsv_fuse_opts* opts, int* nStages, int* stage_gates,
+                                     int capacity) {
+  using namespace qsv;
+  if (!nStages) return fail(QSV_ERROR_INVALID_VALUE, "null nStages");
+  std::vector<int> ops, passes;
+  if (qsv_status st = plan_counts_any(nbQubits, dtype, gates, nGates, op, offset, opts, &ops, &passes))
+    return st;
+  *nStages = (int)ops.size();
   if (stage_gates)
-    for (int i = 0; i < capacity && i < (int)stages.size(); ++i)
-      stage_gates[i] = (int)stages[i].gates.size();
+    for (int i = 0; i < capacity && i < (int)ops.size(); ++i) stage_gates[i] = ops[i];
+  return QSV_SUCCESS;
+}
+
+extern "C" qsv_status qsv_plan_passes(int nbQubits, qsv_dtype dtype, const qsv_gate* gates,
+                                      size_t nGates, char op, int offset,
+                                      const qsv_fuse_opts* opts, int* nStages, int* nPasses,
+                                      int* nOps) {
+  using namespace qsv;
+  if (!nStages || !nPasses || !nOps) return fail(QSV_ERROR_INVALID_VALUE, "null output");
+  std::vector<int> ops, passes;
+  if (qsv_status st = plan_counts_any(nbQubits, dtype, gates, nGates, op, offset, opts, &ops, &passes))
+    return st;
+  *nStages = (int)ops.size();
+  *nPasses = 0;
+  *nOps = 0;
+  for (size_t i = 0; i < ops.size(); ++i) {
+    *nPasses += passes[i];
+    *nOps += ops[i];
+  }
   return QSV_SUCCESS;
 }

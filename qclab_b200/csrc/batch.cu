@@ -12,7 +12,8 @@
 // their tiles through a per-CTA slot of a global workspace.  The stage and
 // pass plans come from the same planner as the single-state fused path
 // (stage_exec.cuh), packed for all circuits into one device buffer.
-// Gradient terms are summed tile by tile by the owning CTA in a fixed order,
+// Gradient terms are summed by warp shuffles into a per-stage shared-memory
+// accumulator and added to the results once per stage, all in a fixed order,
 // so results are deterministic.
 #include <algorithm>
 #include <cmath>
@@ -46,7 +47,7 @@ struct qsv_batch_s {
   cudaStream_t captured_on = nullptr;
   // offsets of the plan sections
   size_t off_jobs = 0, off_stages = 0, off_passes = 0, off_ops = 0, off_coefs = 0,
-         off_runoff = 0, off_groups = 0, off_terms = 0;
+         off_runoff = 0, off_groups = 0, off_terms = 0, off_red = 0;
 };
 
 namespace {
@@ -56,6 +57,8 @@ struct BStage {          // one fused stage of one circuit
   int32_t m, full;
   int32_t pass0, npasses, op0, coef0;  // into the plan arrays (absolute)
   int32_t run0;                        // runoff offset (absolute)
+  int32_t red0, nred;                  // gradient reductions: red_slots[red0..+nred)
+  int32_t nops, ncoef;                 // ops and coefficients (staged in shared memory)
 };
 
 struct BGroup {          // observable term group (terms whose flips fit a tile)
@@ -90,71 +93,14 @@ struct BArgs {
   const uint64_t* runoff;
   const BGroup* groups;
   const BTerm* terms;
+  const int32_t* red_slots;
   void* work;
   size_t work_stride;    // elements per CTA slot (2 vectors)
   double* results;       // [ncirc] energies, then gradients
   unsigned* counter;
   int vec16;
+  int tile_elems;        // 2^M: the shared-memory tiles hold 2 x tile_elems elements
 };
-
-// register passes with a block larger than the pass's thread groups
-// (threads >= 2^(m-R) idle in the pass but join every barrier/reduction)
-template <typename V, int NV, int R, bool FULL>
-__device__ __noinline__ void passes_b(V* t0, V* t1, const BStage& S, const BArgs& a, double2* red,
-                         double* grads) {
-  const PassDev* passes = a.passes + S.pass0;
-  const POp* ops = a.ops + S.op0;
-  const V* coefs = static_cast<const V*>(a.coefs) + S.coef0;
-  const uint32_t groups = 1u << (S.m - R);
-  const bool act = threadIdx.x < groups;
-  for (int pi = 0; pi < S.npasses; ++pi) {
-    const PassDev& P = passes[pi];
-    uint32_t tb = act ? threadIdx.x : 0;
-#pragma unroll
-    for (int k = 0; k < R; ++k) tb = ins0(tb, P.pos[k]);
-    const uint32_t ptb = phys<V>(tb);
-    V x[1 << R], y[1 << R];
-    if (act) {
-#pragma unroll
-      for (int j = 0; j < (1 << R); ++j) {
-        const uint32_t o = ptb ^ P.off[j];
-        x[j] = t0[o];
-        if (NV == 2) y[j] = t1[o];
-      }
-    }
-    for (int o = 0; o < P.nops; ++o) {
-      const POp op = ops[P.op0 + o];
-      if (op.shape == P_RED) {
-        if constexpr (NV == 2 && FULL) {
-          double im = 0.0;
-          if (act) {
-            const double2 s = red_dispatch<V, R>(x, y, op);
-            switch (op.ny & 3) {
-              case 0: im = s.y; break;
-              case 1: im = s.x; break;
-              case 2: im = -s.y; break;
-              default: im = -s.x; break;
-            }
-          }
-          const double2 tot = block_sum(make_double2(op.w * im, 0.0), red);
-          if (threadIdx.x == 0) grads[op.slot] += tot.x;
-        }
-      } else if (act) {
-        apply_reg<V, R, FULL>(x, op, coefs);
-        if (NV == 2) apply_reg<V, R, FULL>(y, op, coefs);
-      }
-    }
-    if (act) {
-#pragma unroll
-      for (int j = 0; j < (1 << R); ++j) {
-        const uint32_t o = ptb ^ P.off[j];
-        t0[o] = x[j];
-        if (NV == 2) t1[o] = y[j];
-      }
-    }
-    __syncthreads();
-  }
-}
 
 template <typename V>
 __device__ __forceinline__ TileArgs stage_tile(const BStage& S, int n, int low,
@@ -166,6 +112,37 @@ __device__ __forceinline__ TileArgs stage_tile(const BStage& S, int n, int low,
   for (int j = 0; j < 32; ++j) ta.bits[j] = S.bits[j];
   ta.runoff = runoff + S.run0;
   return ta;
+}
+
+// One fused stage of a job on psi (NV = 1) or psi and lambda (NV = 2): the
+// stage's plan is staged in shared memory once, then every tile of the stage
+// is swept (the one resident tile of a circuit that fits shared memory).
+// Threads beyond the stage's 2^(m-R) register groups idle in the passes.
+template <typename V, int NV, int R>
+__device__ __forceinline__ void run_stage(const BStage& S, int n, int low, bool single,
+                                          const BArgs& a, V* t0, V* t1, V* psi, V* lam,
+                                          double* racc, unsigned char* plan) {
+  const PassDev* passes;
+  const POp* ops;
+  const V* coefs;
+  stage_plan<V>(plan, a.passes + S.pass0, S.npasses, a.ops + S.op0, S.nops,
+                static_cast<const V*>(a.coefs) + S.coef0, S.ncoef, &passes, &ops, &coefs);
+  __syncthreads();
+  const uint32_t ngroups = 1u << (S.m - R);
+  if (single) {
+    run_passes<V, NV, R, true, 0, true>(t0, t1, passes, S.npasses, ops, coefs, racc, ngroups);
+    return;
+  }
+  const TileArgs ta = stage_tile<V>(S, n, low, a.runoff);
+  const uint64_t ntiles = 1ull << (n - S.m);
+  for (uint64_t t = 0; t < ntiles; ++t) {
+    const uint64_t base = tile_base(ta, t);
+    load_tile<V, NV>(psi, lam, t0, t1, ta, base, a.vec16);
+    __syncthreads();
+    run_passes<V, NV, R, true, 0, true>(t0, t1, passes, S.npasses, ops, coefs, racc, ngroups);
+    store_tile<V, NV>(psi, lam, t0, t1, ta, base, a.vec16);
+    __syncthreads();
+  }
 }
 
 // lambda (+)= H_group psi on a resident tile; returns this thread's
@@ -196,13 +173,22 @@ __device__ __forceinline__ double apply_group(const V* t0, V* t1, const BGroup& 
   return e;
 }
 
+// CTAs per SM the persistent kernel is compiled for: at 1 its ~200 registers
+// per thread need no spills; at 2 it spills about 300 bytes per thread but
+// runs the 4096-circuit batch 14 % faster (measured on a B200).
+#ifndef QSV_BATCH_MINBLOCKS
+#define QSV_BATCH_MINBLOCKS 2
+#endif
+
 template <typename V, int RF, int RB>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, QSV_BATCH_MINBLOCKS)
 k_batch(BArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double2 red[32];
   __shared__ int job_s;
   V* t0 = reinterpret_cast<V*>(smem_raw);
+  double* racc = reinterpret_cast<double*>(smem_raw + size_t(2) * a.tile_elems * sizeof(V));
+  unsigned char* plan = smem_raw + size_t(2) * a.tile_elems * sizeof(V) + kRaccBytes;
   for (;;) {
     if (threadIdx.x == 0) job_s = (int)atomicAdd(a.counter, 1u);
     __syncthreads();
@@ -230,25 +216,9 @@ k_batch(BArgs a) {
     __syncthreads();
 
     // ---- forward ----
-    for (int s = 0; s < J.nfwd; ++s) {
-      const BStage S = a.stages[J.fwd0 + s];
-      if (single) {
-        if (S.full) passes_b<V, 1, RF, true>(t0, t1, S, a, red, grads);
-        else passes_b<V, 1, RF, false>(t0, t1, S, a, red, grads);
-      } else {
-        const TileArgs ta = stage_tile<V>(S, J.n, J.low, a.runoff);
-        const uint64_t ntiles = 1ull << (J.n - S.m);
-        for (uint64_t t = 0; t < ntiles; ++t) {
-          const uint64_t base = tile_base(ta, t);
-          load_tile<V, 1>(psi, nullptr, t0, nullptr, ta, base, a.vec16);
-          __syncthreads();
-          if (S.full) passes_b<V, 1, RF, true>(t0, t1, S, a, red, grads);
-          else passes_b<V, 1, RF, false>(t0, t1, S, a, red, grads);
-          store_tile<V, 1>(psi, nullptr, t0, nullptr, ta, base, a.vec16);
-          __syncthreads();
-        }
-      }
-    }
+    for (int s = 0; s < J.nfwd; ++s)
+      run_stage<V, 1, RF>(a.stages[J.fwd0 + s], J.n, J.low, single, a, t0, t1, psi, lam, racc,
+                          plan);
 
     // ---- lambda = H psi, E = <psi|H|psi> ----
     double e = 0.0;
@@ -292,22 +262,19 @@ k_batch(BArgs a) {
     // ---- backward: uncompute psi and lambda, gradient terms in-tile ----
     for (int s = 0; s < J.nbwd; ++s) {
       const BStage S = a.stages[J.bwd0 + s];
-      if (single) {
-        if (S.full) passes_b<V, 2, RB, true>(t0, t1, S, a, red, grads);
-        else passes_b<V, 2, RB, false>(t0, t1, S, a, red, grads);
-      } else {
-        const TileArgs ta = stage_tile<V>(S, J.n, J.low, a.runoff);
-        const uint64_t ntiles = 1ull << (J.n - S.m);
-        for (uint64_t t = 0; t < ntiles; ++t) {
-          const uint64_t base = tile_base(ta, t);
-          load_tile<V, 2>(psi, lam, t0, t1, ta, base, a.vec16);
-          __syncthreads();
-          if (S.full) passes_b<V, 2, RB, true>(t0, t1, S, a, red, grads);
-          else passes_b<V, 2, RB, false>(t0, t1, S, a, red, grads);
-          store_tile<V, 2>(psi, lam, t0, t1, ta, base, a.vec16);
-          __syncthreads();
+      for (int i = threadIdx.x; i < S.nred * kRedWarps; i += blockDim.x) racc[i] = 0.0;
+      run_stage<V, 2, RB>(S, J.n, J.low, single, a, t0, t1, psi, lam, racc, plan);
+      // the stage's gradient terms, summed over warps in a fixed order by one
+      // thread (parameters may repeat within a stage)
+      if (threadIdx.x == 0) {
+        const int warps = red_warps();
+        for (int r = 0; r < S.nred; ++r) {
+          double t = 0.0;
+          for (int w = 0; w < warps; ++w) t += racc[r * kRedWarps + w];
+          grads[a.red_slots[S.red0 + r]] += t;
         }
       }
+      __syncthreads();
     }
     __syncthreads();
   }
@@ -355,7 +322,7 @@ qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate*
   const int low = (opts && opts->low_bits > 0) ? opts->low_bits : default_low_bits(sizeof(V));
   if (M < RF || M - RB > 8 || M > 14)
     return fail(QSV_ERROR_INVALID_VALUE, "batch tile_bits %d outside [%d, %d]", M, RF, RB + 8);
-  const size_t smem = (size_t(2) << M) * sizeof(V);
+  const size_t smem = (size_t(2) << M) * sizeof(V) + kRaccBytes + kPlanSmemMax;
   if (smem > 200 * 1024) return fail(QSV_ERROR_SIZE, "batch tiles exceed shared memory");
 
   PackedPlan<V> plan;
@@ -428,6 +395,10 @@ qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate*
         S.op0 = (int32_t)ps.op0;
         S.coef0 = (int32_t)ps.coef0;
         S.run0 = (int32_t)ps.run0;
+        S.red0 = (int32_t)ps.red0;
+        S.nred = ps.nred;
+        S.nops = ps.nops;
+        S.ncoef = ps.ncoef;
         stages.push_back(S);
       }
       *count = (int32_t)(stages.size() - *first);
@@ -503,6 +474,7 @@ qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate*
   b->off_runoff = off; off = align(off + plan.runoff.size() * sizeof(uint64_t));
   b->off_groups = off; off = align(off + groups.size() * sizeof(BGroup));
   b->off_terms = off;  off = align(off + terms.size() * sizeof(BTerm));
+  b->off_red = off;    off = align(off + plan.red_slots.size() * sizeof(int32_t));
   std::vector<unsigned char> host(off, 0);
   auto put = [&](size_t o, const void* p, size_t bytes) { if (bytes) std::memcpy(host.data() + o, p, bytes); };
   put(b->off_jobs, jobs.data(), jobs.size() * sizeof(BJob));
@@ -513,6 +485,7 @@ qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate*
   put(b->off_runoff, plan.runoff.data(), plan.runoff.size() * sizeof(uint64_t));
   put(b->off_groups, groups.data(), groups.size() * sizeof(BGroup));
   put(b->off_terms, terms.data(), terms.size() * sizeof(BTerm));
+  put(b->off_red, plan.red_slots.data(), plan.red_slots.size() * sizeof(int32_t));
 
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
@@ -561,11 +534,13 @@ qsv_status launch_batch(qsv_batch_s* b, cudaStream_t stream) {
   a.runoff = reinterpret_cast<const uint64_t*>(p + b->off_runoff);
   a.groups = reinterpret_cast<const BGroup*>(p + b->off_groups);
   a.terms = reinterpret_cast<const BTerm*>(p + b->off_terms);
+  a.red_slots = reinterpret_cast<const int32_t*>(p + b->off_red);
   a.work = b->work;
   a.work_stride = b->work_bytes > 256 ? b->work_bytes / sizeof(V) / b->blocks : 0;
   a.results = b->results;
   a.counter = b->counter;
   a.vec16 = 1;
+  a.tile_elems = 1 << b->tile_bits;
   // zero the results (gradients accumulate) and the work counter
   if (qsv_status st = cuda_status(cudaMemsetAsync(b->results, 0, b->nresults * sizeof(double), stream),
                                   "batch results reset"))

@@ -28,12 +28,14 @@ int default_low_bits(size_t elem_bytes);
 // Plans the items into stages and runs them.
 qsv_status execute_fused(const ExecArgs& x);
 
+// Tile bits the executor uses for nv vectors of an n-qubit state: the
+// requested (or default) size, at most 14 and n, and at most 256 threads of
+// 2^r amplitudes (times the groups a thread takes per pass).
+int effective_tile_bits(size_t elem_bytes, int nv, int n, const qsv_fuse_opts* opts);
+
 // Number of tiles the executor will use for nv vectors of a state.
 inline uint64_t fused_tiles(int n, size_t elem_bytes, int nv, const qsv_fuse_opts* opts) {
-  int m = (opts && opts->tile_bits > 0) ? opts->tile_bits : default_tile_bits(elem_bytes, nv);
-  if (m > 14) m = 14;
-  if (m > n) m = n;
-  return 1ull << (n - m);
+  return 1ull << (n - effective_tile_bits(elem_bytes, nv, n, opts));
 }
 
 // Tiled reductions (reduce.cu).

@@ -5,7 +5,8 @@
 namespace qsv {
 
 std::vector<Stage> plan_stages(const std::vector<Lowered>& gates, int n, int m,
-                               int low, int max_gates) {
+                               int low, int max_gates, int max_red, size_t max_bytes,
+                               size_t elem_bytes) {
   std::vector<Stage> stages;
   if (m > n) m = n;
   if (low > m) low = m;
@@ -22,11 +23,17 @@ std::vector<Stage> plan_stages(const std::vector<Lowered>& gates, int n, int m,
     uint64_t S = lowmask;
     uint64_t blocked = 0;
     Stage st;
+    int nred = 0;
+    size_t bytes = 0;
     rest.clear();
     for (size_t r = 0; r < remaining.size(); ++r) {
       const int gi = remaining[r];
       const uint64_t b = gate_bits(gates[gi]);
-      const bool full = (max_gates > 0 && (int)st.gates.size() >= max_gates);
+      const bool red = gates[gi].shape == SH_RED;
+      const size_t gb = plan_bytes_of(gates[gi], elem_bytes);
+      const bool full = (max_gates > 0 && (int)st.gates.size() >= max_gates) ||
+                        (red && max_red > 0 && nred >= max_red) ||
+                        (max_bytes > 0 && !st.gates.empty() && bytes + gb > max_bytes);
       if (full || (b & blocked)) {
         blocked |= b;
         rest.push_back(gi);
@@ -34,11 +41,15 @@ std::vector<Stage> plan_stages(const std::vector<Lowered>& gates, int n, int m,
       }
       if ((b & ~S) == 0) {
         st.gates.push_back(gi);
+        nred += red;
+        bytes += gb;
         continue;
       }
       if (__builtin_popcountll(S | b) <= m) {
         S |= b;
         st.gates.push_back(gi);
+        nred += red;
+        bytes += gb;
         continue;
       }
       blocked |= b;

@@ -45,11 +45,27 @@ inline uint64_t gate_bits(const Lowered& L) {
   }
 }
 
+// Upper bound of the device plan bytes one item adds to its stage: its op
+// (24 B), a pass descriptor (80 B, as if the op had a pass to itself) and
+// its coefficients of elem_bytes each.
+inline size_t plan_bytes_of(const Lowered& L, size_t elem_bytes) {
+  int nc = 0;
+  switch (L.shape) {
+    case SH_PAIR: case SH_CPAIR: nc = 4; break;
+    case SH_QUAD: nc = 16; break;
+    case SH_HALF: case SH_CHALF: case SH_SWAP: nc = 1; break;
+    default: break;
+  }
+  return 24 + 80 + size_t(nc) * elem_bytes;
+}
+
 // Builds stages for an n-qubit state with tiles of 2^m amplitudes whose
-// lowest `low` bits are contiguous.  max_gates bounds the gates of a stage
-// (0 = unbounded).
+// lowest `low` bits are contiguous.  max_gates bounds the gates of a stage,
+// max_red its gradient reductions (SH_RED items) and max_bytes the plan
+// bytes of its items (plan_bytes_of with elem_bytes); 0 = unbounded.
 std::vector<Stage> plan_stages(const std::vector<Lowered>& gates, int n, int m,
-                               int low, int max_gates);
+                               int low, int max_gates, int max_red = 0,
+                               size_t max_bytes = 0, size_t elem_bytes = 16);
 
 // A register pass inside a stage: r tile bits (ascending local positions)
 // whose 2^r amplitudes one thread holds in registers while it applies the

@@ -27,20 +27,25 @@
 #ifndef QSV_PRECOMP_OFF     // pass offsets precomputed on the host
 #define QSV_PRECOMP_OFF 1
 #endif
-// Measured on a B200 (28-qubit brick, depth 200): complex<double> runs
-// fastest with 8 amplitudes per thread at 3 CTAs per SM, complex<float> with
-// 32 amplitudes per thread at 2 CTAs per SM (at 3 its passes spill).
+// Measured on a B200 (brick circuits, 30 qubits complex<double> and 32
+// qubits complex<float>, plan staged in shared memory): complex<double> runs
+// fastest with 16 amplitudes per thread at 2 CTAs per SM (8 per thread: 5 %
+// slower at 2 CTAs, 20 % at 3, where it spills); complex<float> with 16 per
+// thread at 3 CTAs per SM (32 per thread at 2 CTAs: even).
 #ifndef QSV_RBITS_C128      // register bits of a complex<double> pass
-#define QSV_RBITS_C128 3
+#define QSV_RBITS_C128 4
 #endif
 #ifndef QSV_RBITS_C64       // register bits of a complex<float> (or real) pass
-#define QSV_RBITS_C64 5
+#define QSV_RBITS_C64 4
 #endif
 #ifndef QSV_MINBLOCKS_C128  // CTAs per SM the complex<double> stage kernel targets
-#define QSV_MINBLOCKS_C128 3
+#define QSV_MINBLOCKS_C128 2
 #endif
 #ifndef QSV_MINBLOCKS_C64   // the same for complex<float> and real elements
-#define QSV_MINBLOCKS_C64 2
+#define QSV_MINBLOCKS_C64 3
+#endif
+#ifndef QSV_TURN_BITS_C128  // log2 register groups per thread and pass (complex<double>)
+#define QSV_TURN_BITS_C128 0
 #endif
 
 namespace qsv {
@@ -69,9 +74,29 @@ struct POp {
   uint8_t mmask, mval;  // MUL: x *= c where (j & mmask) == mval; RED: projector
   uint8_t zy;       // RED: sign mask
   int16_t coef;     // stage-relative index of the first coefficient
-  int16_t pad;
+  int16_t ridx;     // RED: index among the stage's reductions (< kMaxRed)
   int32_t slot;     // RED: output row
 };
+
+// Gradient reductions of a stage accumulate per warp in shared memory,
+// racc[ridx * kRedWarps + warp] (a warp-shuffle sum, no block barrier), and
+// are summed over the warps once per tile or stage in a fixed order.
+constexpr int kMaxRed = 64;    // reductions per stage (the planner's cap)
+constexpr int kRedWarps = 8;   // warps of a 256-thread block
+constexpr size_t kRaccBytes = size_t(kMaxRed) * kRedWarps * sizeof(double);
+
+// `lanes` (a power of two <= 32) threads of the warp take part: fewer than
+// 32 only when the block, or its working part, is smaller than a warp.
+__device__ __forceinline__ void red_accumulate(double v, int ridx, double* racc, unsigned lanes) {
+  const unsigned mask = lanes >= 32 ? 0xffffffffu : ((1u << lanes) - 1u);
+  for (unsigned o = 16; o > 0; o >>= 1)
+    if (o < lanes) v += __shfl_xor_sync(mask, v, o);
+  if ((threadIdx.x & 31) == 0) racc[ridx * kRedWarps + (threadIdx.x >> 5)] += v;
+}
+
+__device__ __forceinline__ int red_warps() { return (int)((blockDim.x + 31) >> 5); }
+
+
 
 struct PassDev {
   int8_t pos[8];    // local tile bits of the pass, ascending
@@ -82,6 +107,47 @@ struct PassDev {
   // over GF(2) in the index bits
   uint16_t off[32];
 };
+
+static_assert(sizeof(PassDev) == 80, "PassDev layout");
+static_assert(sizeof(POp) == 20, "POp layout");
+
+// A stage's plan (pass descriptors, ops, coefficients) is copied into shared
+// memory once per CTA: every thread reads every op and coefficient, and from
+// global memory those reads were the kernel's main latency stall.  The
+// planner keeps a stage's plan within kPlanSmemMax bytes.
+constexpr size_t kPlanSmemMax = 16384;
+
+__host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
+
+template <typename V>
+__host__ __device__ inline size_t plan_smem_bytes(int npasses, int nops, int ncoef) {
+  return align16(size_t(npasses) * sizeof(PassDev)) + align16(size_t(nops) * sizeof(POp)) +
+         align16(size_t(ncoef) * sizeof(V));
+}
+
+// Copies `bytes` (a multiple of 4) from global to shared memory.
+__device__ __forceinline__ void copy_words(void* dst, const void* src, size_t bytes) {
+  uint32_t* d = static_cast<uint32_t*>(dst);
+  const uint32_t* s = static_cast<const uint32_t*>(src);
+  for (size_t i = threadIdx.x; i < bytes / 4; i += blockDim.x) d[i] = __ldg(s + i);
+}
+
+// Stages the plan at `dst` (16-byte aligned); returns the three section
+// pointers.  The caller synchronises the block before use.
+template <typename V>
+__device__ __forceinline__ void stage_plan(unsigned char* dst, const PassDev* passes, int npasses,
+                                           const POp* ops, int nops, const V* coefs, int ncoef,
+                                           const PassDev** sp, const POp** so, const V** sc) {
+  unsigned char* pp = dst;
+  unsigned char* po = pp + align16(size_t(npasses) * sizeof(PassDev));
+  unsigned char* pc = po + align16(size_t(nops) * sizeof(POp));
+  copy_words(pp, passes, size_t(npasses) * sizeof(PassDev));
+  copy_words(po, ops, size_t(nops) * sizeof(POp));
+  copy_words(pc, coefs, size_t(ncoef) * sizeof(V));
+  *sp = reinterpret_cast<const PassDev*>(pp);
+  *so = reinterpret_cast<const POp*>(po);
+  *sc = reinterpret_cast<const V*>(pc);
+}
 
 // Host copy of the swizzle (see phys<V> below) for `epu` elements per unit.
 inline uint32_t phys_host(uint32_t e, uint32_t epu) {
@@ -234,6 +300,29 @@ __device__ __forceinline__ void ctl_dispatch(V (&x)[1 << R], int p, int q, int c
 }
 
 // Quads (j, j|1<<P0, j|1<<P1, j|both), P0 > P1, in apply4's slot order.
+// Coefficient read at its point of use (not hoisted out of the quad loop, so
+// the 16 coefficients of a dense 4x4 op never occupy registers together).
+__device__ __forceinline__ double2 ld_use(const double2* p) {
+  double2 r;
+  asm volatile("ld.v2.f64 {%0, %1}, [%2];" : "=d"(r.x), "=d"(r.y) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ float2 ld_use(const float2* p) {
+  float2 r;
+  asm volatile("ld.v2.f32 {%0, %1}, [%2];" : "=f"(r.x), "=f"(r.y) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ double ld_use(const double* p) {
+  double r;
+  asm volatile("ld.f64 %0, [%1];" : "=d"(r) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ float ld_use(const float* p) {
+  float r;
+  asm volatile("ld.f32 %0, [%1];" : "=f"(r) : "l"(p));
+  return r;
+}
+
 template <typename V, int R, int P0, int P1>
 __device__ __forceinline__ void quad_reg(V (&x)[1 << R], int form, int mul, const V* __restrict__ c) {
   constexpr int m0 = 1 << P0, m1 = 1 << P1;
@@ -255,8 +344,9 @@ __device__ __forceinline__ void quad_reg(V (&x)[1 << R], int form, int mul, cons
       V y[4];
 #pragma unroll
       for (int r = 0; r < 4; ++r)
-        y[r] = mac(mac(mac(scale1(c[4 * r], x0), c[4 * r + 1], x1), c[4 * r + 2], x2),
-                   c[4 * r + 3], x3);
+        y[r] = mac(mac(mac(scale1(ld_use(c + 4 * r), x0), ld_use(c + 4 * r + 1), x1),
+                       ld_use(c + 4 * r + 2), x2),
+                   ld_use(c + 4 * r + 3), x3);
       x[j] = y[0]; x[j | m0] = y[1]; x[j | m1] = y[2]; x[j | m0 | m1] = y[3];
     }
 }
@@ -440,14 +530,40 @@ __device__ __forceinline__ void store_tile(V* __restrict__ v0, V* __restrict__ v
   }
 }
 
+// Two adjacent 8-byte elements (a 16-byte aligned unit) as one access; only
+// instantiated for 8-byte element types.
+template <typename V>
+__device__ __forceinline__ void ld_pair(const V* p, V& a, V& b) {
+  if constexpr (sizeof(V) == 8) {
+    struct alignas(16) U { V a, b; };
+    const U u = *reinterpret_cast<const U*>(p);
+    a = u.a;
+    b = u.b;
+  } else {
+    a = p[0];
+    b = p[1];
+  }
+}
+template <typename V>
+__device__ __forceinline__ void st_pair(V* p, const V& a, const V& b) {
+  if constexpr (sizeof(V) == 8) {
+    struct alignas(16) U { V a, b; };
+    *reinterpret_cast<U*>(p) = U{a, b};
+  } else {
+    p[0] = a;
+    p[1] = b;
+  }
+}
+
 // Shared-memory offset of register j of a pass: from the host-computed
-// pattern offsets (QSV_PRECOMP_OFF) or recomputed from the pass bits.
+// pattern offsets (QSV_PRECOMP_OFF) or recomputed from the pass bits.  The
+// pass descriptor may sit in shared or global memory (plain loads only).
 template <typename V, int R>
 __device__ __forceinline__ uint32_t pass_off(uint32_t ptb, uint32_t tb, const uint16_t* poff,
                                              const int8_t* pos, int j) {
 #if QSV_PRECOMP_OFF
   (void)tb; (void)pos;
-  return ptb ^ __ldg(poff + j);
+  return ptb ^ poff[j];
 #else
   (void)ptb; (void)poff;
   uint32_t e = tb;
@@ -459,24 +575,46 @@ __device__ __forceinline__ uint32_t pass_off(uint32_t ptb, uint32_t tb, const ui
 }
 
 // Runs the register passes of one stage on a resident tile (t0, t1).  RED
-// results: sink(slot, value) is called by thread 0 with the block's sum.
-template <typename V, int NV, int R, bool FULL, typename Sink>
+// results accumulate into racc (see red_accumulate); every thread of the
+// block runs the op loop, so the warp shuffles see full warps.
+// A pass has ngroups = 2^(m-R) register groups.  Normally the block has one
+// thread per group; with TURN a smaller block takes them in turns (every
+// thread the same number), with PART a larger block leaves threads
+// >= ngroups idle (they still reach every barrier).
+template <typename V, int NV, int R, bool FULL, int TURN = 0, bool PART = false>
 __device__ __forceinline__ void run_passes(V* t0, V* t1, const PassDev* __restrict__ passes,
                                            int npasses, const POp* __restrict__ ops,
-                                           const V* __restrict__ coefs, double2* red, Sink sink) {
+                                           const V* __restrict__ coefs, double* racc,
+                                           uint32_t ngroups) {
+  const uint32_t ng = (TURN || PART) ? ngroups : blockDim.x;
+  const unsigned lanes = PART ? (ngroups < 32u ? ngroups : 32u)
+                              : (blockDim.x < 32u ? blockDim.x : 32u);
   for (int pi = 0; pi < npasses; ++pi) {
     const PassDev& P = passes[pi];
-    uint32_t tb = threadIdx.x;
+   for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x) {
+    uint32_t tb = g;
 #pragma unroll
     for (int k = 0; k < R; ++k) tb = ins0(tb, P.pos[k]);
     const uint32_t ptb = phys<V>(tb);
     const uint16_t* __restrict__ poff = P.off;
     V x[1 << R], y[1 << R];
+    // 8-byte elements with element bit 0 in the pass: registers 2i and 2i+1
+    // are the two halves of one 16-byte unit, moved as one access
+    const bool pairs = sizeof(V) == 8 && P.pos[0] == 0;
+    if (pairs) {
 #pragma unroll
-    for (int j = 0; j < (1 << R); ++j) {
-      const uint32_t o = pass_off<V, R>(ptb, tb, poff, P.pos, j);
-      x[j] = t0[o];
-      if (NV == 2) y[j] = t1[o];
+      for (int j = 0; j < (1 << R); j += 2) {
+        const uint32_t o = pass_off<V, R>(ptb, tb, poff, P.pos, j);
+        ld_pair(t0 + o, x[j], x[j + 1]);
+        if (NV == 2) ld_pair(t1 + o, y[j], y[j + 1]);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < (1 << R); ++j) {
+        const uint32_t o = pass_off<V, R>(ptb, tb, poff, P.pos, j);
+        x[j] = t0[o];
+        if (NV == 2) y[j] = t1[o];
+      }
     }
     for (int o = 0; o < P.nops; ++o) {
       const POp op = ops[P.op0 + o];
@@ -490,30 +628,45 @@ __device__ __forceinline__ void run_passes(V* t0, V* t1, const PassDev* __restri
             case 2: im = -s.y; break;
             default: im = -s.x; break;
           }
-          const double2 tot = block_sum(make_double2(op.w * im, 0.0), red);
-          if (threadIdx.x == 0) sink(op.slot, tot.x);
+          red_accumulate(op.w * im, op.ridx, racc, lanes);
         }
       } else {
         apply_reg<V, R, FULL>(x, op, coefs);
         if (NV == 2) apply_reg<V, R, FULL>(y, op, coefs);
       }
     }
+    if (pairs) {
 #pragma unroll
-    for (int j = 0; j < (1 << R); ++j) {
-      const uint32_t o = pass_off<V, R>(ptb, tb, poff, P.pos, j);
-      t0[o] = x[j];
-      if (NV == 2) t1[o] = y[j];
+      for (int j = 0; j < (1 << R); j += 2) {
+        const uint32_t o = pass_off<V, R>(ptb, tb, poff, P.pos, j);
+        st_pair(t0 + o, x[j], x[j + 1]);
+        if (NV == 2) st_pair(t1 + o, y[j], y[j + 1]);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < (1 << R); ++j) {
+        const uint32_t o = pass_off<V, R>(ptb, tb, poff, P.pos, j);
+        t0[o] = x[j];
+        if (NV == 2) t1[o] = y[j];
+      }
     }
+   }
     __syncthreads();
   }
 }
 
 // register bits per pass: 2^R amplitudes (x NV vectors) per thread
-template <typename V> constexpr int reg_bits(int nv) {
+template <typename V> __host__ __device__ constexpr int reg_bits(int nv) {
   return sizeof(V) >= 16 ? (nv == 2 ? 3 : QSV_RBITS_C128) : (nv == 2 ? 4 : QSV_RBITS_C64);
 }
-template <typename V> constexpr int min_blocks() {
-  return sizeof(V) >= 16 ? QSV_MINBLOCKS_C128 : QSV_MINBLOCKS_C64;
+// Two-vector (adjoint) sweeps keep 2 CTAs per SM: their passes hold twice the
+// amplitudes and spill at the complex<double> single-vector target.
+// log2 of the register groups each thread takes per pass (single-vector sweeps)
+template <typename V> __host__ __device__ constexpr int turn_bits(int nv) {
+  return (nv == 1 && sizeof(V) >= 16) ? QSV_TURN_BITS_C128 : 0;
+}
+template <typename V, int NV> __host__ __device__ constexpr int min_blocks() {
+  return NV == 2 ? 2 : (sizeof(V) >= 16 ? QSV_MINBLOCKS_C128 : QSV_MINBLOCKS_C64);
 }
 
 // ---- host: packing a plan ---------------------------------------------------
@@ -530,6 +683,9 @@ struct PackedStage {
   int full;  // has dense 4x4 ops or gradient reductions (needs the full kernel)
   int bits[64];
   size_t pass0, npasses, op0, run0, coef0;
+  size_t red0;  // the stage's reductions: red_slots[red0 .. red0 + nred)
+  int nred;
+  int nops, ncoef;  // the stage's ops and coefficients
 };
 
 template <typename V>
@@ -538,6 +694,7 @@ struct PackedPlan {
   std::vector<POp> ops;
   std::vector<V> coefs;
   std::vector<uint64_t> runoff;
+  std::vector<int32_t> red_slots;  // output row of each reduction, by stage
   std::vector<PackedStage> stages;
 };
 

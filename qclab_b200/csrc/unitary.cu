@@ -138,12 +138,13 @@ template <typename VA, typename VB>
 qsv_status nrmf_typed(qsv_state_s* a, qsv_state_s* b, double* out) {
   const uint64_t N = dim(a->n);
   const unsigned blocks = blocks_for(N);
-  // [blocks] maxima | scale | pad | [blocks] double2 sums | total
-  const size_t bytes = (blocks + 2) * sizeof(double) + (blocks + 1) * sizeof(double2);
+  // [blocks] maxima | scale | pad to 16 B | [blocks] double2 sums | total
+  const size_t sum_off = ((blocks + 1) * sizeof(double) + 15) & ~size_t(15);
+  const size_t bytes = sum_off + (blocks + 1) * sizeof(double2);
   if (qsv_status st = ensure_scratch(a, bytes)) return st;
   double* pmax = static_cast<double*>(a->scratch);
   double* scale = pmax + blocks;
-  double2* psum = reinterpret_cast<double2*>(pmax + blocks + 2);
+  double2* psum = reinterpret_cast<double2*>(static_cast<unsigned char*>(a->scratch) + sum_off);
   const VA* da = static_cast<const VA*>(a->d);
   const VB* db = static_cast<const VB*>(b->d);
   k_diff_max<VA, VB><<<blocks, kThreads, 0, a->stream>>>(da, db, N, pmax);

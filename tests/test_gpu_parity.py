@@ -162,6 +162,25 @@ def test_host_apply_entry_point(cuda):
     assert np.max(np.abs(w - v)) < 1e-15
 
 
+def test_circuit_offset_and_nesting(cuda):
+    """QCircuit::apply adds offset_ + offset to every gate (QCircuit.hpp:130-143),
+    for a top-level circuit with an offset and for nested sub-circuits."""
+    from qclab_b200 import QCircuit
+    sub = W.random_mixed(3, 25, seed=4)
+    sub.setOffset(2)
+    top = QCircuit(6)
+    top.push_back(W.random_mixed(6, 10, seed=5))
+    top.push_back(sub)
+    rng = np.random.default_rng(3)
+    x = (rng.normal(size=64) + 1j * rng.normal(size=64)).astype(np.complex128)
+    for op in ("N", "C"):
+        for circ, off in ((sub, 1), (top, 0)):
+            got = x.copy()
+            circ.apply(op, 6, got, off)
+            recs = circ.gate_records(np.complex128, offset=off)
+            assert np.array_equal(got, oracle.ref_apply(x, recs, op))
+
+
 def test_wrap_caller_owned_device_memory(cuda):
     """simulate_device(T*): the library works in place on caller memory."""
     import torch
