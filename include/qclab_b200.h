@@ -151,7 +151,11 @@ typedef struct qsv_fuse_opts {
   int reg_bits;      /* k: qubits per register block inside a tile           */
   int max_stage_gates;
   int profile;       /* 1: time every stage with CUDA events (see below)   */
-  int reserved[3];
+  int engine;        /* complex single-vector sweeps: 0 = every register pass
+                        of 2 tile bits multiplied out into a 4x4 complex
+                        matrix and applied on the FP64 tensor cores (default);
+                        1 = sparse register passes on the CUDA cores          */
+  int reserved[2];
 } qsv_fuse_opts;
 
 /* Fused path: the gate list is planned into stages; each stage streams the

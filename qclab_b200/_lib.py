@@ -14,7 +14,8 @@ from pathlib import Path
 import numpy as np
 
 _PKG = Path(__file__).resolve().parent
-LIB_PATH = _PKG / "libqclab_b200.so"
+# QCLAB_B200_LIB selects another build of the library (no in-place build then)
+LIB_PATH = Path(os.environ.get("QCLAB_B200_LIB", _PKG / "libqclab_b200.so"))
 
 # ---- enums (mirror include/qclab_b200.h) ----------------------------------
 SUCCESS = 0
@@ -50,7 +51,8 @@ class Gate(C.Structure):
 class FuseOpts(C.Structure):
     """``qsv_fuse_opts``."""
     _fields_ = [("tile_bits", C.c_int), ("low_bits", C.c_int), ("reg_bits", C.c_int),
-                ("max_stage_gates", C.c_int), ("profile", C.c_int), ("reserved", C.c_int * 3)]
+                ("max_stage_gates", C.c_int), ("profile", C.c_int), ("engine", C.c_int),
+                ("reserved", C.c_int * 2)]
 
 
 class BatchOpts(C.Structure):
@@ -137,7 +139,7 @@ def load(build_if_missing: bool = True):
     with _lock:
         if _lib is not None:
             return _lib
-        if build_if_missing:
+        if build_if_missing and "QCLAB_B200_LIB" not in os.environ:
             from . import build as _build
             _build.build()
         if not LIB_PATH.exists():

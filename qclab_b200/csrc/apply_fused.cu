@@ -14,6 +14,8 @@
 // path for complex<double>, not bitwise: the planner reorders commuting
 // gates, which changes rounding).
 #include <algorithm>
+#include <complex>
+#include <initializer_list>
 #include <cstring>
 #include <vector>
 #include "fused.hpp"
@@ -37,9 +39,75 @@ int8_t classify(const Lowered& L, bool cplx) {
   return F_GENERIC;
 }
 
+using cplxd = std::complex<double>;
+
+// Host mirror of apply_reg: op on the 2^R amplitudes of one register group,
+// with FP64 coefficients c (the same semantics as pair2f / quad_reg /
+// the P_MUL loop).
+void host_apply_pop(std::vector<cplxd>& x, int R, const POp& op, const cplxd* c) {
+  const int N = 1 << R;
+  switch (op.shape) {
+    case P_PAIR:
+    case P_CPAIR: {
+      const int mt = 1 << op.p0;
+      const int cm = op.shape == P_CPAIR ? (1 << op.p1) : 0;
+      const int cv = op.shape == P_CPAIR ? (op.cval << op.p1) : 0;
+      for (int j = 0; j < N; ++j) {
+        if ((j & mt) || (j & cm) != cv) continue;
+        const cplxd x1 = x[j], x2 = x[j | mt];
+        if (op.form == F_PERM) {
+          x[j] = x2;
+          x[j | mt] = x1;
+        } else {
+          x[j] = c[0] * x1 + c[1] * x2;
+          x[j | mt] = c[2] * x1 + c[3] * x2;
+        }
+      }
+      break;
+    }
+    case P_MUL:
+      for (int j = 0; j < N; ++j)
+        if ((j & op.mmask) == op.mval) x[j] *= c[0];
+      break;
+    case P_QUAD: {
+      const int m0 = 1 << op.p0, m1 = 1 << op.p1;
+      for (int j = 0; j < N; ++j) {
+        if ((j & m0) || (j & m1)) continue;
+        if (op.form == F_PERM) {
+          const cplxd xb = x[j | m0], xc = x[j | m1];
+          x[j | m0] = op.mul ? c[0] * xc : xc;
+          x[j | m1] = op.mul ? c[0] * xb : xb;
+        } else {
+          const cplxd in[4] = {x[j], x[j | m0], x[j | m1], x[j | m0 | m1]};
+          cplxd y[4];
+          for (int rr = 0; rr < 4; ++rr)
+            y[rr] = c[4 * rr] * in[0] + c[4 * rr + 1] * in[1] + c[4 * rr + 2] * in[2] +
+                    c[4 * rr + 3] * in[3];
+          x[j] = y[0];
+          x[j | m0] = y[1];
+          x[j | m1] = y[2];
+          x[j | m0 | m1] = y[3];
+        }
+      }
+      break;
+    }
+    default:
+      break;
+  }
+}
+
+template <typename V> V dense_coef(cplxd z);
+template <> double2 dense_coef<double2>(cplxd z) { return make_double2(z.real(), z.imag()); }
+template <> float2 dense_coef<float2>(cplxd z) {
+  return make_float2((float)z.real(), (float)z.imag());
+}
+template <> double dense_coef<double>(cplxd z) { return z.real(); }
+template <> float dense_coef<float>(cplxd z) { return (float)z.real(); }
+
 template <typename V>
 qsv_status pack_plan(const std::vector<Lowered>& gates, int n, int m, int low, int r,
-                     int max_gates, PackedPlan<V>* out) {
+                     int max_gates, PackedPlan<V>* out, int dense_min, size_t plan_cap) {
+  const int min_ops = dense_min >= 0 ? dense_min : QSV_DENSE_MIN_OPS;
   constexpr bool cplx = Elem<V>::cplx;
   std::vector<Stage> stages =
       plan_stages(gates, n, m, low, max_gates, kMaxRed, kPlanSmemMax, sizeof(V));
@@ -68,11 +136,24 @@ qsv_status pack_plan(const std::vector<Lowered>& gates, int n, int m, int low, i
     std::vector<uint32_t> op_bits;
     for (int gi : stg.gates) op_bits.push_back(local_mask(gate_bits(gates[gi])));
     std::vector<Pass> pl = plan_passes(op_bits, stg.m, r);
-    for (const Pass& p : pl) {
-      PassDev pd{};
+    // Phase 1: every pass packed sparse into its own buffers (op.coef
+    // relative to the pass), with its coefficients also kept in FP64.
+    struct PassBuf {
+      PassDev pd;
+      int r;
+      std::vector<POp> ops;
+      std::vector<V> coefs;
+      std::vector<cplxd> c64;
+      bool red = false;
+    };
+    std::vector<PassBuf> bufs(pl.size());
+    for (size_t pi = 0; pi < pl.size(); ++pi) {
+      const Pass& p = pl[pi];
+      PassBuf& B = bufs[pi];
+      B.r = p.r;
+      PassDev& pd = B.pd;
+      pd = PassDev{};
       for (int k = 0; k < 8; ++k) pd.pos[k] = (k < p.r) ? (int8_t)p.pos[k] : 0;
-      pd.op0 = (int32_t)(out->ops.size() - ps.op0);
-      pd.nops = (int32_t)p.ops.size();
       for (int j = 0; j < (1 << p.r) && j < 32; ++j) {
         uint32_t pat = 0;
         for (int k = 0; k < p.r; ++k)
@@ -93,9 +174,7 @@ qsv_status pack_plan(const std::vector<Lowered>& gates, int n, int m, int low, i
       for (int oi : p.ops) {
         const Lowered& L = gates[stg.gates[oi]];
         POp op{};
-        if (out->coefs.size() - ps.coef0 > 30000)
-          return fail(QSV_ERROR_SIZE, "fused stage too large");
-        op.coef = (int16_t)(out->coefs.size() - ps.coef0);
+        op.coef = (int16_t)B.coefs.size();
         int nc = 0;
         switch (L.shape) {
           case SH_PAIR:
@@ -146,20 +225,69 @@ qsv_status pack_plan(const std::vector<Lowered>& gates, int n, int m, int low, i
             if (ps.nred >= kMaxRed) return fail(QSV_ERROR_INVALID_VALUE, "internal: stage reductions");
             op.ridx = (int16_t)ps.nred++;
             out->red_slots.push_back(L.slot);
+            B.red = true;
             break;
           }
           default:
             return fail(QSV_ERROR_INVALID_VALUE, "internal: shape %d in a fused stage", L.shape);
         }
-        for (int i = 0; i < nc; ++i) out->coefs.push_back(host_coef<V>(L.m, i));
-        out->ops.push_back(op);
+        for (int i = 0; i < nc; ++i) {
+          B.coefs.push_back(host_coef<V>(L.m, i));
+          B.c64.push_back(cplx ? cplxd(L.m[2 * i], L.m[2 * i + 1]) : cplxd(L.m[2 * i], 0.0));
+        }
+        B.ops.push_back(op);
       }
-      out->passes.push_back(pd);
+    }
+    // Phase 2: multiply passes out into one dense 2^r x 2^r op (no gradient
+    // terms, enough ops) while the stage's plan stays within its budget.
+    size_t nops_total = 0, ncoef_total = 0;
+    for (const PassBuf& B : bufs) {
+      nops_total += B.ops.size();
+      ncoef_total += B.coefs.size();
+    }
+    for (PassBuf& B : bufs) {
+      const int N = 1 << B.r;
+      if (min_ops <= 0 || B.r != r || r > QSV_DENSE_MAX_R || B.red || (int)B.ops.size() < min_ops)
+        continue;
+      const size_t nops_after = nops_total - B.ops.size() + 1;
+      const size_t ncoef_after = ncoef_total - B.coefs.size() + size_t(N) * N;
+      if (plan_smem_bytes<V>((int)bufs.size(), (int)nops_after, (int)ncoef_after) > plan_cap)
+        continue;
+      std::vector<cplxd> U(size_t(N) * N);  // column-major: U[k * N + i]
+      std::vector<cplxd> x(N);
+      for (int k = 0; k < N; ++k) {
+        std::fill(x.begin(), x.end(), cplxd(0.0, 0.0));
+        x[k] = 1.0;
+        for (const POp& q : B.ops) host_apply_pop(x, B.r, q, B.c64.data() + q.coef);
+        for (int i = 0; i < N; ++i) U[size_t(k) * N + i] = x[i];
+      }
+      POp d{};
+      d.shape = P_DENSE;
+      d.coef = 0;
+      B.ops.assign(1, d);
+      B.coefs.clear();
+      for (const cplxd& z : U) B.coefs.push_back(dense_coef<V>(z));
+      nops_total = nops_after;
+      ncoef_total = ncoef_after;
+    }
+    // Phase 3: append (op.coef and PassDev.op0 relative to the stage).
+    for (PassBuf& B : bufs) {
+      if (out->coefs.size() - ps.coef0 + B.coefs.size() > 30000)
+        return fail(QSV_ERROR_SIZE, "fused stage too large");
+      B.pd.op0 = (int32_t)(out->ops.size() - ps.op0);
+      B.pd.nops = (int32_t)B.ops.size();
+      const int16_t cbase = (int16_t)(out->coefs.size() - ps.coef0);
+      for (POp q : B.ops) {
+        q.coef = (int16_t)(q.coef + cbase);
+        out->ops.push_back(q);
+      }
+      out->coefs.insert(out->coefs.end(), B.coefs.begin(), B.coefs.end());
+      out->passes.push_back(B.pd);
     }
     ps.npasses = out->passes.size() - ps.pass0;
     ps.nops = (int)(out->ops.size() - ps.op0);
     ps.ncoef = (int)(out->coefs.size() - ps.coef0);
-    if (plan_smem_bytes<V>((int)ps.npasses, ps.nops, ps.ncoef) > kPlanSmemMax)
+    if (plan_smem_bytes<V>((int)ps.npasses, ps.nops, ps.ncoef) > plan_cap)
       return fail(QSV_ERROR_INVALID_VALUE, "internal: stage plan exceeds its shared-memory budget");
     tile_runoffs(stg.bits, stg.m, low, &out->runoff);
     out->stages.push_back(ps);
@@ -167,10 +295,10 @@ qsv_status pack_plan(const std::vector<Lowered>& gates, int n, int m, int low, i
   return QSV_SUCCESS;
 }
 
-template qsv_status pack_plan<double2>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<double2>*);
-template qsv_status pack_plan<float2>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<float2>*);
-template qsv_status pack_plan<double>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<double>*);
-template qsv_status pack_plan<float>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<float>*);
+template qsv_status pack_plan<double2>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<double2>*, int, size_t);
+template qsv_status pack_plan<float2>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<float2>*, int, size_t);
+template qsv_status pack_plan<double>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<double>*, int, size_t);
+template qsv_status pack_plan<float>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<float>*, int, size_t);
 
 }  // namespace fx
 
@@ -255,6 +383,331 @@ void* pick_kernel(int r, bool full) {
   return stage_kernel<V, NV, 1>(full);
 }
 
+// ---- dense register passes on the FP64 tensor cores ------------------------
+// Every register pass of a stage acts on 2 tile bits with one 4x4 complex
+// matrix U (the product of its gates, formed on the host in FP64).  A warp
+// takes 32 groups of 4 amplitudes at a time (a "chunk") and applies the 8x8
+// real matrix M = [[Re U, -Im U], [Im U, Re U]] to their (re; im) vectors
+// with mma.sync m8n8k4 f64: per 8-group column tile, D = A0 B0 + A1 B1 with
+//   A_s[r][k] = M[r][4s + k]          lane: r = lane / 4, k = lane % 4
+//   B_s[k][g] = (s ? im : re) of amplitude k of group g     (g = lane / 4)
+//   D[r][g]   -> lane: r = lane / 4, g = 2 (lane % 4) + {0, 1}
+// (row r < 4: real part of output amplitude r, r >= 4: imaginary part of
+// amplitude r - 4).  Amplitudes are read and written in shared memory in
+// their storage type and computed in FP64.  The tile bit insertion and the
+// shared-memory swizzle are linear over GF(2), so the address of (group,
+// amplitude) is the XOR of a chunk part and per-lane parts.
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b,
+                                            double c0, double c1) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%4, %5};"
+               : "=d"(d0), "=d"(d1)
+               : "d"(a), "d"(b), "d"(c0), "d"(c1));
+}
+
+struct DmmaArgs {
+  TileArgs ta;
+  int npasses, nops, ncoef;
+  const PassDev* passes;
+  const POp* ops;
+  const double2* coefs;  // per pass: U column-major (U[i][k] at k * 4 + i)
+  int vec16;
+};
+
+template <typename V>
+__global__ void __launch_bounds__(256, 3) k_dmma(V* __restrict__ v0, DmmaArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t size = 1u << a.ta.m;
+  V* t0 = reinterpret_cast<V*>(smem_raw);
+  const PassDev* passes;
+  const POp* ops;
+  const double2* coefs;
+  stage_plan<double2>(smem_raw + size_t(size) * sizeof(V), a.passes, a.npasses, a.ops, a.nops,
+                      a.coefs, a.ncoef, &passes, &ops, &coefs);
+  const uint64_t base = tile_base(a.ta, blockIdx.x);
+  load_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int q = lane >> 2, k4 = lane & 3;
+  const bool im_row = q >= 4;
+  const uint32_t nchunks = size >> 7;  // 32 groups x 4 amplitudes
+  for (int pi = 0; pi < a.npasses; ++pi) {
+    const PassDev& P = passes[pi];
+    const uint16_t* T = P.off;  // address tables (dmma_tables)
+    const double2 u = coefs[ops[P.op0].coef + k4 * 4 + (q & 3)];  // U[q % 4][k4]
+    const double a0 = im_row ? u.y : u.x;
+    const double a1 = im_row ? u.x : -u.y;
+    // input (group q, amplitude k4); output (amplitude q % 4, group 2 k4 +
+    // im_row) after the real/imaginary exchange between lanes l and l ^ 16
+    const uint32_t in_lane = (uint32_t)T[4 + q] ^ T[12 + k4];
+    const uint32_t out_lane = (uint32_t)T[4 + 2 * k4 + (im_row ? 1 : 0)] ^ T[12 + (q & 3)];
+    uint32_t col[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) col[t] = T[t];
+    for (uint32_t c = warp; c < nchunks; c += nwarps) {
+      uint32_t cb = 0;
+      for (uint32_t cc = c, k = 0; cc; cc >>= 1, ++k)
+        if (cc & 1u) cb ^= T[16 + k];
+      double b0[4], b1[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const double2 xv = to_d2(t0[cb ^ col[t] ^ in_lane]);
+        b0[t] = xv.x;
+        b1[t] = xv.y;
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        double d0, d1;
+        dmma_m8n8k4(d0, d1, a0, b0[t], 0.0, 0.0);
+        dmma_m8n8k4(d0, d1, a1, b1[t], d0, d1);
+        // lane l < 16 holds the real parts of amplitude q for groups 2k4 and
+        // 2k4 + 1, lane l ^ 16 the imaginary parts: swap one value each
+        const double recv = __shfl_xor_sync(0xffffffffu, im_row ? d0 : d1, 16);
+        t0[cb ^ col[t] ^ out_lane] =
+            from_d2<V>(im_row ? make_double2(recv, d1) : make_double2(d0, recv));
+      }
+    }
+    __syncthreads();
+  }
+  store_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
+}
+
+// Three-bit passes: the 8x8 complex U as the 16x16 real matrix M (rows /
+// columns 0-7: real parts of amplitudes 0-7, 8-15: imaginary parts); per
+// 8-group column tile and row half h, D_h = sum_s A_hs B_s over 4 k-steps
+//   A_hs[r][k] = M[8h + r][4s + k],  B_s[k][g] = row 4s + k of group g,
+// so one lane ends with the real (h = 0) and imaginary (h = 1) parts of the
+// same output amplitude q for groups 2k4 and 2k4 + 1: 32 MMAs per chunk of
+// 32 groups x 8 amplitudes, one 16-byte store per output.
+template <typename V>
+__global__ void __launch_bounds__(256, 2) k_dmma3(V* __restrict__ v0, DmmaArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t size = 1u << a.ta.m;
+  V* t0 = reinterpret_cast<V*>(smem_raw);
+  const PassDev* passes;
+  const POp* ops;
+  const double2* coefs;
+  stage_plan<double2>(smem_raw + size_t(size) * sizeof(V), a.passes, a.npasses, a.ops, a.nops,
+                      a.coefs, a.ncoef, &passes, &ops, &coefs);
+  const uint64_t base = tile_base(a.ta, blockIdx.x);
+  load_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int q = lane >> 2, k4 = lane & 3;
+  const uint32_t nchunks = size >> 8;  // 32 groups x 8 amplitudes
+  for (int pi = 0; pi < a.npasses; ++pi) {
+    const PassDev& P = passes[pi];
+    const uint16_t* T = P.off;
+    const double2* U = coefs + ops[P.op0].coef;        // U[i][k] at k * 8 + i
+    const double2 ulo = U[k4 * 8 + q], uhi = U[(4 + k4) * 8 + q];
+    double A[2][4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const double2 uu = (s & 1) ? uhi : ulo;
+      A[0][s] = (s < 2) ? uu.x : -uu.y;   // real output row
+      A[1][s] = (s < 2) ? uu.y : uu.x;    // imaginary output row
+    }
+    const uint32_t in0 = (uint32_t)T[4 + q] ^ T[12 + k4];
+    const uint32_t in1 = (uint32_t)T[4 + q] ^ T[12 + 4 + k4];
+    const uint32_t out0 = (uint32_t)T[4 + 2 * k4] ^ T[12 + q];
+    const uint32_t out1 = (uint32_t)T[4 + 2 * k4 + 1] ^ T[12 + q];
+    for (uint32_t c = warp; c < nchunks; c += nwarps) {
+      uint32_t cb = 0;
+      for (uint32_t cc = c, k = 0; cc; cc >>= 1, ++k)
+        if (cc & 1u) cb ^= T[20 + k];
+      double B[4][4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const uint32_t tb = cb ^ T[t];
+        const double2 x0 = to_d2(t0[tb ^ in0]), x1 = to_d2(t0[tb ^ in1]);
+        B[t][0] = x0.x;  // real part of amplitude k4
+        B[t][1] = x1.x;  // real part of amplitude 4 + k4
+        B[t][2] = x0.y;
+        B[t][3] = x1.y;
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        double re0 = 0.0, re1 = 0.0, im0 = 0.0, im1 = 0.0;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          dmma_m8n8k4(re0, re1, A[0][s], B[t][s], re0, re1);
+          dmma_m8n8k4(im0, im1, A[1][s], B[t][s], im0, im1);
+        }
+        const uint32_t tb = cb ^ T[t];
+        t0[tb ^ out0] = from_d2<V>(make_double2(re0, im0));
+        t0[tb ^ out1] = from_d2<V>(make_double2(re1, im1));
+      }
+    }
+    __syncthreads();
+  }
+  store_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
+}
+
+// Rank over GF(2) of up to four 4-bit vectors.
+int gf2_rank(std::initializer_list<uint32_t> in) {
+  uint32_t v[4];
+  int k = 0;
+  for (uint32_t x : in) v[k++] = x;
+  int r = 0;
+  for (int bit = 3; bit >= 0; --bit) {
+    int piv = -1;
+    for (int i = r; i < k; ++i)
+      if ((v[i] >> bit) & 1u) { piv = i; break; }
+    if (piv < 0) continue;
+    std::swap(v[r], v[piv]);
+    for (int i = 0; i < k; ++i)
+      if (i != r && ((v[i] >> bit) & 1u)) v[i] ^= v[r];
+    ++r;
+  }
+  return r;
+}
+
+// Address tables of one tensor-core pass on R = 2 or 3 tile bits p0 < p1
+// (< p2) of an m-bit tile (epu elements per 16-byte unit), in PassDev.off:
+//   off[t]          t < 4     group part of column tile t   (group bits 3, 4)
+//   off[4 + g]      g < 8     group part of column g         (group bits 0..2)
+//   off[12 + j]     j < 2^R   amplitude part of amplitude j  (pass bits)
+//   off[12+2^R + k] k         chunk part of chunk bit k      (group bits 5..)
+// all as swizzled shared-memory element offsets (phys is linear, so the
+// address of (chunk, tile, column, amplitude) is the XOR of its parts).
+// Group index bits map to the tile's other bits; the three lowest are chosen
+// so that the shared-memory banks a quarter-warp (16-byte elements) or
+// half-warp (8-byte elements) touches on load and on store are independent
+// of the banks of the pass bits p0, p1 that vary within it.
+void dmma_tables(PassDev* P, int R, int m, int epu) {
+  const int nb = R;
+  int pos[3] = {P->pos[0], P->pos[1], R == 3 ? P->pos[2] : -1};
+  const uint32_t bank_mask = epu == 1 ? 7u : 15u;
+  auto dir = [&](int b) { return (uint32_t)phys_host(1u << b, (uint32_t)epu) & bank_mask; };
+  std::vector<int> rest;
+  for (int b = 0; b < m; ++b)
+    if (b != pos[0] && b != pos[1] && b != pos[2]) rest.push_back(b);
+  const uint32_t u = dir(pos[0]), v = dir(pos[1]);
+  const int top = epu == 1 ? 6 : 8;
+  int best = -1, s0 = rest[0], s1 = rest[1], s2 = rest[2];
+  for (size_t i0 = 0; i0 < rest.size() && best < top; ++i0)
+    for (size_t i1 = 0; i1 < rest.size() && best < top; ++i1)
+      for (size_t i2 = 0; i2 < rest.size() && best < top; ++i2) {
+        const int b0 = rest[i0], b1 = rest[i1], b2 = rest[i2];
+        if (b0 == b1 || b0 == b2 || b1 == b2) continue;
+        const int score = epu == 1
+            ? gf2_rank({dir(b0), u, v}) + gf2_rank({u, dir(b1), dir(b2)})
+            : gf2_rank({dir(b0), dir(b1), u, v}) + gf2_rank({u, v, dir(b1), dir(b2)});
+        if (score > best) { best = score; s0 = b0; s1 = b1; s2 = b2; }
+      }
+  std::vector<int> sel = {s0, s1, s2};
+  for (int b : rest)
+    if (b != s0 && b != s1 && b != s2) sel.push_back(b);
+  auto map = [&](uint32_t g) {
+    uint32_t e = 0;
+    for (size_t i = 0; i < sel.size(); ++i)
+      if ((g >> i) & 1u) e |= 1u << sel[i];
+    return e;
+  };
+  auto ph = [&](uint32_t e) { return (uint16_t)phys_host(e, (uint32_t)epu); };
+  for (int t = 0; t < 4; ++t) P->off[t] = ph(map(8u * t));
+  for (int g = 0; g < 8; ++g) P->off[4 + g] = ph(map((uint32_t)g));
+  const int na = 1 << nb;
+  for (int j = 0; j < na; ++j) {
+    uint32_t e = 0;
+    for (int k = 0; k < nb; ++k)
+      if ((j >> k) & 1) e |= 1u << pos[k];
+    P->off[12 + j] = ph(e);
+  }
+  for (int k = 0; k + 5 + nb < m && 12 + na + k < 32; ++k) P->off[12 + na + k] = ph(map(32u << k));
+}
+
+// Single-vector sweep of a complex state on the tensor-core engine; returns
+// QSV_ERROR_NOT_SUPPORTED (nothing launched) when the plan does not fit it.
+template <typename V>
+qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool vec16) {
+  qsv_state_s* s = x.s;
+  const int n = s->n;
+  const int R = (QSV_DMMA_BITS == 3 && m >= 8) ? 3 : 2;
+  PackedPlan<double2> plan;
+  // plans sized per launch: a few KB typically, at most kDmmaPlanMax
+  constexpr size_t kDmmaPlanMax = 96 * 1024;
+  if ((size_t(1) << m) * sizeof(V) + kDmmaPlanMax > 200 * 1024) return QSV_ERROR_NOT_SUPPORTED;
+  if (qsv_status st = pack_plan<double2>(*x.items, n, m, low, R, max_gates, &plan, 1, kDmmaPlanMax))
+    return st;
+  if (plan.stages.empty()) return QSV_SUCCESS;
+  for (const PackedStage& ps : plan.stages)
+    for (size_t pi = ps.pass0; pi < ps.pass0 + ps.npasses; ++pi) {
+      PassDev& P = plan.passes[pi];
+      if (P.nops != 1 || plan.ops[ps.op0 + P.op0].shape != P_DENSE || ps.m < 5 + R)
+        return QSV_ERROR_NOT_SUPPORTED;
+      dmma_tables(&P, R, ps.m, Units<V>::per);
+    }
+  auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
+  const size_t pass_bytes = plan.passes.size() * sizeof(PassDev);
+  const size_t op_off = align(pass_bytes);
+  const size_t coef_off = align(op_off + plan.ops.size() * sizeof(POp));
+  const size_t run_off = align(coef_off + plan.coefs.size() * sizeof(double2));
+  const size_t total = run_off + plan.runoff.size() * sizeof(uint64_t);
+  std::vector<unsigned char> host(total);
+  std::memcpy(host.data(), plan.passes.data(), pass_bytes);
+  std::memcpy(host.data() + op_off, plan.ops.data(), plan.ops.size() * sizeof(POp));
+  std::memcpy(host.data() + coef_off, plan.coefs.data(), plan.coefs.size() * sizeof(double2));
+  std::memcpy(host.data() + run_off, plan.runoff.data(), plan.runoff.size() * sizeof(uint64_t));
+  if (qsv_status st = ensure_scratch(s, total)) return st;
+  unsigned char* dev = static_cast<unsigned char*>(s->scratch);
+  if (qsv_status st = cuda_status(cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice,
+                                                  s->stream), "dense plan upload"))
+    return st;
+  void* kern = R == 3 ? (void*)k_dmma3<V> : (void*)k_dmma<V>;
+  if (qsv_status st = cuda_status(cudaFuncSetAttribute(kern,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       200 * 1024), "dense stage shared-memory attribute"))
+    return st;
+  const uint64_t ntiles = 1ull << (n - m);
+  if (x.ntiles_out) *x.ntiles_out = ntiles;
+  const bool profile = x.opts && x.opts->profile;
+  std::vector<cudaEvent_t> ev;
+  if (profile) {
+    ev.resize(plan.stages.size() + 1);
+    for (auto& e : ev)
+      if (qsv_status st = cuda_status(cudaEventCreate(&e), "cudaEventCreate")) return st;
+    cudaEventRecord(ev[0], s->stream);
+  }
+  V* p0 = static_cast<V*>(x.v0);
+  for (size_t si = 0; si < plan.stages.size(); ++si) {
+    const PackedStage& ps = plan.stages[si];
+    DmmaArgs a;
+    a.ta.n = n;
+    a.ta.m = ps.m;
+    a.ta.low = low;
+    for (int j = 0; j < 64; ++j) a.ta.bits[j] = (int8_t)ps.bits[j];
+    a.ta.runoff = reinterpret_cast<const uint64_t*>(dev + run_off) + ps.run0;
+    a.npasses = (int)ps.npasses;
+    a.nops = ps.nops;
+    a.ncoef = ps.ncoef;
+    a.passes = reinterpret_cast<const PassDev*>(dev) + ps.pass0;
+    a.ops = reinterpret_cast<const POp*>(dev + op_off) + ps.op0;
+    a.coefs = reinterpret_cast<const double2*>(dev + coef_off) + ps.coef0;
+    a.vec16 = vec16 ? 1 : 0;
+    const size_t smem_stage =
+        (size_t(1) << ps.m) * sizeof(V) + plan_smem_bytes<double2>((int)ps.npasses, ps.nops, ps.ncoef);
+    void* args[] = {&p0, &a};
+    if (qsv_status st = cuda_status(cudaLaunchKernel(kern, dim3((unsigned)ntiles),
+                                                     dim3(256), args, smem_stage, s->stream),
+                                    "dense stage launch"))
+      return st;
+    count_launch();
+    if (profile) cudaEventRecord(ev[si + 1], s->stream);
+  }
+  if (profile) {
+    qsv_status st = cuda_status(cudaEventSynchronize(ev.back()), "stage timing synchronize");
+    g_stage_ms.clear();
+    for (size_t si = 0; si < plan.stages.size() && !st; ++si) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[si], ev[si + 1]);
+      g_stage_ms.push_back(ms);
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (st) return st;
+  }
+  return QSV_SUCCESS;
+}
+
 template <typename V>
 qsv_status execute_typed(const ExecArgs& x) {
   constexpr int EPU = Units<V>::per;
@@ -276,6 +729,22 @@ qsv_status execute_typed(const ExecArgs& x) {
   const bool vec16 = (low >= log_epu) && (m >= log_epu) &&
                      (reinterpret_cast<uintptr_t>(x.v0) % 16 == 0) &&
                      (x.nv == 1 || reinterpret_cast<uintptr_t>(x.v1) % 16 == 0);
+
+  // complex single-vector sweeps run on the tensor-core engine unless the
+  // caller asks for sparse passes; tiles need at least one 128-amplitude chunk
+  if constexpr (Elem<V>::cplx) {
+    const int engine = opts ? opts->engine : 0;
+    // its tiles have no per-thread register limit: the requested or default
+    // size, at most 14 bits, n and the shared memory
+    int md = (opts && opts->tile_bits > 0) ? opts->tile_bits : default_tile_bits(sizeof(V), 1);
+    md = std::min(std::min(md, 14), n);
+    while (md > 7 && (size_t(1) << md) * sizeof(V) + 96 * 1024 > 200 * 1024) --md;
+    const int lowd = std::min(low, md);
+    if (x.nv == 1 && x.nslots == 0 && engine == 0 && md >= 7) {
+      const qsv_status st = execute_dmma<V>(x, md, lowd, max_gates, vec16);
+      if (st != QSV_ERROR_NOT_SUPPORTED) return st;
+    }
+  }
 
   PackedPlan<V> plan;
   if (qsv_status st = pack_plan<V>(*x.items, n, m, low, r, max_gates, &plan)) return st;

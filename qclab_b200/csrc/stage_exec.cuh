@@ -44,6 +44,20 @@
 #ifndef QSV_MINBLOCKS_C64   // the same for complex<float> and real elements
 #define QSV_MINBLOCKS_C64 3
 #endif
+// A register pass whose ops (no gradient terms) number at least
+// QSV_DENSE_MIN_OPS is multiplied out on the host into one dense 2^R x 2^R
+// matrix (P_DENSE) when R <= QSV_DENSE_MAX_R: 2^R complex MACs per amplitude
+// in place of the ops' dispatch and predicates.  0 disables.
+#ifndef QSV_DENSE_MIN_OPS
+#define QSV_DENSE_MIN_OPS 3
+#endif
+#ifndef QSV_DENSE_MAX_R
+#define QSV_DENSE_MAX_R 3
+#endif
+// Tile bits per register pass of the tensor-core engine (2 or 3).
+#ifndef QSV_DMMA_BITS
+#define QSV_DMMA_BITS 3
+#endif
 #ifndef QSV_TURN_BITS_C128  // log2 register groups per thread and pass (complex<double>)
 #define QSV_TURN_BITS_C128 0
 #endif
@@ -60,7 +74,7 @@ enum Form : int8_t {
   F_NEG = 5       // P_MUL by -1 on one control/target pattern (CZ)
 };
 
-enum POpShape : int8_t { P_PAIR = 1, P_CPAIR = 2, P_MUL = 3, P_QUAD = 4, P_RED = 5 };
+enum POpShape : int8_t { P_PAIR = 1, P_CPAIR = 2, P_MUL = 3, P_QUAD = 4, P_RED = 5, P_DENSE = 6 };
 
 // One op of a register pass; positions index the pass's register bits.
 struct POp {
@@ -380,9 +394,29 @@ __device__ __forceinline__ void quad_dispatch_perm(V (&x)[1 << R], int p0, int p
 
 // FULL = false compiles out the dense 4x4 path (the host only sends stages
 // without dense quads and gradient reductions to that kernel).
+// x <- U x for the pass's dense matrix U, stored column by column
+// (c[k * 2^R + i] = U[i][k]): 2^R independent accumulators, one column of
+// coefficients live at a time.
+template <typename V, int R>
+__device__ __forceinline__ void dense_reg(V (&x)[1 << R], const V* __restrict__ c) {
+  constexpr int N = 1 << R;
+  V y[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) y[i] = scale1(c[i], x[0]);
+#pragma unroll
+  for (int k = 1; k < N; ++k)
+#pragma unroll
+    for (int i = 0; i < N; ++i) y[i] = mac(y[i], c[k * N + i], x[k]);
+#pragma unroll
+  for (int i = 0; i < N; ++i) x[i] = y[i];
+}
+
 template <typename V, int R, bool FULL>
 __device__ __forceinline__ void apply_reg(V (&x)[1 << R], const POp& op, const V* __restrict__ cf) {
   switch (op.shape) {
+    case P_DENSE:
+      if constexpr (R <= QSV_DENSE_MAX_R) dense_reg<V, R>(x, cf + op.coef);
+      break;
     case P_PAIR: {
       V c[4];
 #pragma unroll
@@ -700,9 +734,13 @@ struct PackedPlan {
 
 // Plans `gates` for an n-qubit state (tiles of 2^m, `low` contiguous bits,
 // register passes of r bits) and appends the packed stages to `out`.
+// dense_min: passes with at least this many ops (and no gradient terms) are
+// multiplied out into one dense op; -1 = QSV_DENSE_MIN_OPS, 0 = never.
+// plan_cap bounds a stage's plan bytes in shared memory.
 template <typename V>
 qsv_status pack_plan(const std::vector<Lowered>& gates, int n, int m, int low, int r,
-                     int max_gates, PackedPlan<V>* out);
+                     int max_gates, PackedPlan<V>* out, int dense_min = -1,
+                     size_t plan_cap = kPlanSmemMax);
 
 }  // namespace fx
 }  // namespace qsv

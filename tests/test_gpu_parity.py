@@ -82,8 +82,12 @@ def test_fused_matches_reference_within_tolerance(states, dtype):
     for cname, n, recs, op, off, x in circuit_cases(dtype):
         xn = x / np.linalg.norm(x)
         ref = oracle.apply(xn.astype(dtype), recs, op, off)
-        for opts in (None, L.FuseOpts(tile_bits=4, low_bits=2), L.FuseOpts(tile_bits=6, low_bits=1),
-                     L.FuseOpts(tile_bits=12, low_bits=5, max_stage_gates=3)):
+        # engine 0 (tensor-core dense passes, complex states with tiles of
+        # >= 7 bits) and engine 1 (sparse register passes)
+        for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(tile_bits=4, low_bits=2),
+                     L.FuseOpts(tile_bits=6, low_bits=1), L.FuseOpts(tile_bits=7, low_bits=2),
+                     L.FuseOpts(tile_bits=12, low_bits=5, max_stage_gates=3),
+                     L.FuseOpts(tile_bits=12, low_bits=5, max_stage_gates=3, engine=1)):
             y = run_gpu(states, n, dtype, recs, op, off, xn.astype(dtype), fused=True, opts=opts)
             err = np.max(np.abs(y - ref))
             assert err <= tol(dtype), (cname, opts and opts.tile_bits, err)
@@ -102,8 +106,9 @@ def test_random_mixed_large(states, dtype, n):
         ref = oracle.apply(x.copy(), recs, op)
         y = run_gpu(states, n, dtype, recs, op, 0, x)
         assert np.array_equal(y, ref)
-        yf = run_gpu(states, n, dtype, recs, op, 0, x, fused=True)
-        assert np.max(np.abs(yf - ref)) <= tol(dtype)
+        for opts in (None, L.FuseOpts(engine=1)):
+            yf = run_gpu(states, n, dtype, recs, op, 0, x, fused=True, opts=opts)
+            assert np.max(np.abs(yf - ref)) <= tol(dtype), (op, opts and opts.engine)
 
 
 def test_qft20_config(states):
