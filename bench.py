@@ -444,7 +444,10 @@ def main():
     ms_per_step = ms / args.steps
     value = job_throughput(ngates, args.steps, ms, world)
 
-    # roofline of the dominant kernel (the fused stage sweep)
+    # roofline of the dominant kernel: the fused stage sweep, which runs its
+    # register passes on the FP64 tensor cores (k_dmma3).  HBM: one read and
+    # one write of the state per stage launch.  Tensor: each pass applies a
+    # 16x16 real matrix to every 8-amplitude group, 64 flops per amplitude.
     n_stages = len(stage_ms) // max(args.steps, 1)
     state_bytes = (1 << n) * 16
     alg_bytes = 2 * state_bytes
@@ -452,11 +455,22 @@ def main():
     achieved = alg_bytes / (avg_stage_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
     traffic = traffic_per_launch(n, 16)
-    roofline = {"bound": "hbm", "kernel": "k_stage2<double2> (fused stage sweep)",
+    st_, ps_, op_ = C.c_int(), C.c_int(), C.c_int()
+    L.check(lib.qsv_plan_passes(n, L.C128, C.c_void_p(recs.ctypes.data), len(recs), b"N", 0,
+                                None, C.byref(st_), C.byref(ps_), C.byref(op_)), "qsv_plan_passes")
+    flops_step = ps_.value * (1 << n) * 64.0
+    tc_peak = C.c_double()
+    L.check(lib.qsv_fp64_mma_peak(C.byref(tc_peak)), "qsv_fp64_mma_peak")
+    tc_achieved = flops_step / (sum(stage_ms) / max(args.steps, 1) / 1e3) / 1e12
+    roofline = {"bound": "hbm", "kernel": "k_dmma3<double2> (fused stage sweep, FP64 tensor cores)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} hbm_gbs", "traffic": traffic,
                 "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_stage_ms,
-                "launches_per_step": n_stages}
+                "launches_per_step": n_stages,
+                "tensor_fp64": {"achieved": tc_achieved, "peak": tc_peak.value, "unit": "TFLOP/s",
+                                "frac": tc_achieved / tc_peak.value,
+                                "peak_source": "measured live (qsv_fp64_mma_peak, mma.sync m8n8k4 f64)",
+                                "flops_per_step": flops_step, "passes_per_step": ps_.value}}
 
     # unfused reference-exact path on the first layer (side measurement)
     unf = None

@@ -171,7 +171,9 @@ qsv_status qsv_apply_fused(qsv_state state, const qsv_gate* gates,
 qsv_status qsv_last_stage_times(float* ms, int capacity, int* count);
 
 /* Plan statistics for a gate list (no device work): number of stages and
- * of gates per stage.  stage_gates may be NULL.                            */
+ * of ops per stage -- gates for the sparse engine (opts->engine = 1), one
+ * dense matrix per register pass for the tensor-core engine.  stage_gates
+ * may be NULL.                                                             */
 qsv_status qsv_plan_stats(int nbQubits, qsv_dtype dtype, const qsv_gate* gates,
                           size_t nGates, char op, int offset,
                           const qsv_fuse_opts* opts, int* nStages,
@@ -283,6 +285,12 @@ qsv_status qsv_batch_results(qsv_batch batch, void* cuda_stream,
 qsv_status qsv_batch_info(qsv_batch batch, int* blocks, int* threads,
                           int* tile_bits, size_t* workspace_bytes);
 qsv_status qsv_batch_destroy(qsv_batch batch);
+
+/* ---- device probe (new) --------------------------------------------------
+ * FP64 tensor-core throughput of the current device in TFLOP/s (mma.sync
+ * m8n8k4 f64, a few ms): the peak the fused complex sweep is measured
+ * against.  Allocates and frees a small buffer.                            */
+qsv_status qsv_fp64_mma_peak(double* tflops);
 
 /* ---- unitaries ---------------------------------------------------------------
  * A 2^n x 2^n matrix lives on the device in a state object of 2n qubits

@@ -125,6 +125,7 @@ def _declare(lib):
         "qsv_set_identity": ([p], i),
         "qsv_apply_matrix": ([p, gp, sz, C.c_char, C.c_char, i, i], i),
         "qsv_nrmF": ([p, p, C.POINTER(d)], i),
+        "qsv_fp64_mma_peak": ([C.POINTER(d)], i),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)

@@ -14,9 +14,11 @@
 // path for complex<double>, not bitwise: the planner reorders commuting
 // gates, which changes rounding).
 #include <algorithm>
+#include <array>
 #include <complex>
 #include <initializer_list>
 #include <cstring>
+#include <unordered_map>
 #include <vector>
 #include "fused.hpp"
 #include "stage_exec.cuh"
@@ -573,7 +575,28 @@ int gf2_rank(std::initializer_list<uint32_t> in) {
 // so that the shared-memory banks a quarter-warp (16-byte elements) or
 // half-warp (8-byte elements) touches on load and on store are independent
 // of the banks of the pass bits p0, p1 that vary within it.
+void dmma_tables_compute(PassDev* P, int R, int m, int epu);
+
+// The tables depend only on (pass bits, tile bits, element size); passes of
+// a circuit repeat a few patterns, so they are cached per host thread.
 void dmma_tables(PassDev* P, int R, int m, int epu) {
+  thread_local std::unordered_map<uint64_t, std::array<uint16_t, 32>> cache;
+  const uint64_t key = (uint64_t)(uint8_t)P->pos[0] | ((uint64_t)(uint8_t)P->pos[1] << 8) |
+                       ((uint64_t)(uint8_t)(R == 3 ? P->pos[2] : 0xff) << 16) |
+                       ((uint64_t)m << 24) | ((uint64_t)epu << 32) | ((uint64_t)R << 40);
+  auto it = cache.find(key);
+  if (it == cache.end()) {
+    if (cache.size() > 4096) cache.clear();
+    PassDev tmp = *P;
+    dmma_tables_compute(&tmp, R, m, epu);
+    std::array<uint16_t, 32> t;
+    std::memcpy(t.data(), tmp.off, sizeof(tmp.off));
+    it = cache.emplace(key, t).first;
+  }
+  std::memcpy(P->off, it->second.data(), sizeof(P->off));
+}
+
+void dmma_tables_compute(PassDev* P, int R, int m, int epu) {
   const int nb = R;
   int pos[3] = {P->pos[0], P->pos[1], R == 3 ? P->pos[2] : -1};
   const uint32_t bank_mask = epu == 1 ? 7u : 15u;
@@ -616,16 +639,32 @@ void dmma_tables(PassDev* P, int R, int m, int epu) {
   for (int k = 0; k + 5 + nb < m && 12 + na + k < 32; ++k) P->off[12 + na + k] = ph(map(32u << k));
 }
 
+constexpr size_t kDmmaPlanMax = 96 * 1024;  // a tensor-core stage's plan bytes, at most
+
+// Tile bits of the tensor-core engine for an n-qubit complex sweep, or -1
+// when it does not apply (real elements, engine 1, tiles under 2^(5+R)).
+// Its tiles have no per-thread register limit: the requested or default
+// size, at most 14 bits, n and the shared memory.
+template <typename V>
+int dmma_tile_bits(int n, const qsv_fuse_opts* opts) {
+  if (!Elem<V>::cplx || (opts && opts->engine == 1)) return -1;
+  int md = (opts && opts->tile_bits > 0) ? opts->tile_bits : default_tile_bits(sizeof(V), 1);
+  md = std::min(std::min(md, 14), n);
+  while (md > 7 && (size_t(1) << md) * sizeof(V) + kDmmaPlanMax > 200 * 1024) --md;
+  return md >= 7 ? md : -1;
+}
+
+int dmma_pass_bits(int m) { return (QSV_DMMA_BITS == 3 && m >= 8) ? 3 : 2; }
+
 // Single-vector sweep of a complex state on the tensor-core engine; returns
 // QSV_ERROR_NOT_SUPPORTED (nothing launched) when the plan does not fit it.
 template <typename V>
 qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool vec16) {
   qsv_state_s* s = x.s;
   const int n = s->n;
-  const int R = (QSV_DMMA_BITS == 3 && m >= 8) ? 3 : 2;
+  const int R = dmma_pass_bits(m);
   PackedPlan<double2> plan;
   // plans sized per launch: a few KB typically, at most kDmmaPlanMax
-  constexpr size_t kDmmaPlanMax = 96 * 1024;
   if ((size_t(1) << m) * sizeof(V) + kDmmaPlanMax > 200 * 1024) return QSV_ERROR_NOT_SUPPORTED;
   if (qsv_status st = pack_plan<double2>(*x.items, n, m, low, R, max_gates, &plan, 1, kDmmaPlanMax))
     return st;
@@ -732,16 +771,10 @@ qsv_status execute_typed(const ExecArgs& x) {
 
   // complex single-vector sweeps run on the tensor-core engine unless the
   // caller asks for sparse passes; tiles need at least one 128-amplitude chunk
-  if constexpr (Elem<V>::cplx) {
-    const int engine = opts ? opts->engine : 0;
-    // its tiles have no per-thread register limit: the requested or default
-    // size, at most 14 bits, n and the shared memory
-    int md = (opts && opts->tile_bits > 0) ? opts->tile_bits : default_tile_bits(sizeof(V), 1);
-    md = std::min(std::min(md, 14), n);
-    while (md > 7 && (size_t(1) << md) * sizeof(V) + 96 * 1024 > 200 * 1024) --md;
-    const int lowd = std::min(low, md);
-    if (x.nv == 1 && x.nslots == 0 && engine == 0 && md >= 7) {
-      const qsv_status st = execute_dmma<V>(x, md, lowd, max_gates, vec16);
+  if (x.nv == 1 && x.nslots == 0) {
+    const int md = dmma_tile_bits<V>(n, opts);
+    if (md > 0) {
+      const qsv_status st = execute_dmma<V>(x, md, std::min(low, md), max_gates, vec16);
       if (st != QSV_ERROR_NOT_SUPPORTED) return st;
     }
   }
@@ -890,6 +923,20 @@ namespace {
 template <typename V>
 qsv_status plan_counts(const std::vector<Lowered>& low, int n, const qsv_fuse_opts* opts,
                        std::vector<int>* ops, std::vector<int>* passes) {
+  const int md = dmma_tile_bits<V>(n, opts);
+  if (md > 0) {  // the tensor-core engine's plan (its ops are the passes' matrices)
+    const int lowb = std::min((opts && opts->low_bits > 0) ? opts->low_bits : default_low_bits(sizeof(V)), md);
+    const int max_gates = (opts && opts->max_stage_gates > 0) ? opts->max_stage_gates : 256;
+    fx::PackedPlan<double2> plan;
+    if (qsv_status st = fx::pack_plan<double2>(low, n, md, lowb, dmma_pass_bits(md), max_gates, &plan, 1,
+                                               kDmmaPlanMax))
+      return st;
+    for (const fx::PackedStage& ps : plan.stages) {
+      ops->push_back(ps.nops);
+      passes->push_back((int)ps.npasses);
+    }
+    return QSV_SUCCESS;
+  }
   const int m = effective_tile_bits(sizeof(V), 1, n, opts);
   const int lowb = (opts && opts->low_bits > 0) ? opts->low_bits : default_low_bits(sizeof(V));
   const int max_gates = (opts && opts->max_stage_gates > 0) ? opts->max_stage_gates : 256;

@@ -50,13 +50,21 @@ def plan(n, recs, dtype=L.C128, op=b"N", offset=0, opts=None, cap=4096):
 
 
 def test_planner_covers_every_gate_once():
+    lib = L.load()
     for n, depth in [(8, 5), (20, 10), (30, 4)]:
         c = W.brick(n, depth, seed=1)
         recs = c.gate_records(np.complex128)
-        st, ns, sg = plan(n, recs)
+        # sparse register passes: one op per gate
+        st, ns, sg = plan(n, recs, opts=L.FuseOpts(engine=1))
         assert st == 0
         assert sum(sg) == len(recs)
         assert ns <= len(recs)
+        # tensor-core engine: one dense op per pass, no more passes than gates
+        stages, passes, ops = C.c_int(), C.c_int(), C.c_int()
+        assert lib.qsv_plan_passes(n, L.C128, C.c_void_p(recs.ctypes.data), len(recs), b"N", 0,
+                                   None, C.byref(stages), C.byref(passes), C.byref(ops)) == 0
+        assert ops.value == passes.value <= len(recs)
+        assert 0 < stages.value <= passes.value
 
 
 def test_planner_errors_are_status_codes():
