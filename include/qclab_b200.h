@@ -151,10 +151,13 @@ typedef struct qsv_fuse_opts {
   int reg_bits;      /* k: qubits per register block inside a tile           */
   int max_stage_gates;
   int profile;       /* 1: time every stage with CUDA events (see below)   */
-  int engine;        /* complex single-vector sweeps: 0 = every register pass
-                        of 2 tile bits multiplied out into a 4x4 complex
-                        matrix and applied on the FP64 tensor cores (default);
-                        1 = sparse register passes on the CUDA cores          */
+  int engine;        /* complex single-vector sweeps: 0 (default) = every
+                        register pass of 3 tile bits multiplied out into an
+                        8x8 complex matrix and applied on the tensor cores --
+                        FP64 MMA for complex<double>, TF32 MMA with the
+                        three-term split (FP32 accuracy) for complex<float>;
+                        1 = sparse register passes on the CUDA cores;
+                        2 = FP64 MMA for complex<float> too                  */
   int reserved[2];
 } qsv_fuse_opts;
 

@@ -17,6 +17,7 @@
 #include <array>
 #include <complex>
 #include <initializer_list>
+#include <type_traits>
 #include <cstring>
 #include <unordered_map>
 #include <vector>
@@ -544,6 +545,101 @@ __global__ void __launch_bounds__(256, 2) k_dmma3(V* __restrict__ v0, DmmaArgs a
   store_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
 }
 
+// complex<float> passes of three tile bits on the TF32 tensor cores with the
+// three-term split: each operand x = hi + lo (hi = tf32(x), lo = tf32(x - hi))
+// and D += A_lo B_hi + A_hi B_lo + A_hi B_hi in FP32 (the lo*lo term, ~2^-22
+// relative, is dropped), mma.sync m16n8k8 tf32: 24 MMAs per chunk of 32
+// groups x 8 amplitudes.  Fragment lanes as in k_dmma3 (g = lane / 4 is the
+// column group and output amplitude, t = lane % 4 the input amplitudes t and
+// t + 4), so the same address tables serve.
+__device__ __forceinline__ uint32_t tf32_of(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  hi = tf32_of(x);
+  lo = tf32_of(x - __uint_as_float(hi));
+}
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+      "{%8, %9}, {%0, %1, %2, %3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__global__ void __launch_bounds__(256, 2) k_tf32x3(float2* __restrict__ v0, DmmaArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t size = 1u << a.ta.m;
+  float2* t0 = reinterpret_cast<float2*>(smem_raw);
+  const PassDev* passes;
+  const POp* ops;
+  const double2* coefs;
+  stage_plan<double2>(smem_raw + size_t(size) * sizeof(float2), a.passes, a.npasses, a.ops,
+                      a.nops, a.coefs, a.ncoef, &passes, &ops, &coefs);
+  const uint64_t base = tile_base(a.ta, blockIdx.x);
+  load_tile<float2, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const uint32_t nchunks = size >> 8;  // 32 groups x 8 amplitudes
+  for (int pi = 0; pi < a.npasses; ++pi) {
+    const PassDev& P = passes[pi];
+    const uint16_t* T = P.off;
+    const double2* U = coefs + ops[P.op0].coef;  // U[i][k] at k * 8 + i
+    const double2 u0 = U[t * 8 + g], u4 = U[(t + 4) * 8 + g];
+    // A fragments of k-step s: rows g (real out) and g + 8 (imaginary out),
+    // columns t and t + 4 of the real (s = 0) or imaginary (s = 1) inputs
+    float av[2][4];
+    av[0][0] = (float)u0.x;  av[0][1] = (float)u0.y;  av[0][2] = (float)u4.x;  av[0][3] = (float)u4.y;
+    av[1][0] = (float)-u0.y; av[1][1] = (float)u0.x;  av[1][2] = (float)-u4.y; av[1][3] = (float)u4.x;
+    uint32_t ahi[2][4], alo[2][4];
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) split_tf32(av[s][j], ahi[s][j], alo[s][j]);
+    const uint32_t in0 = (uint32_t)T[4 + g] ^ T[12 + t];
+    const uint32_t in1 = (uint32_t)T[4 + g] ^ T[12 + 4 + t];
+    const uint32_t out0 = (uint32_t)T[4 + 2 * t] ^ T[12 + g];
+    const uint32_t out1 = (uint32_t)T[4 + 2 * t + 1] ^ T[12 + g];
+    for (uint32_t c = warp; c < nchunks; c += nwarps) {
+      uint32_t cb = 0;
+      for (uint32_t cc = c, k = 0; cc; cc >>= 1, ++k)
+        if (cc & 1u) cb ^= T[20 + k];
+      float2 x0[4], x1[4];
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const uint32_t tb = cb ^ T[nt];
+        x0[nt] = t0[tb ^ in0];  // amplitude t of column group g
+        x1[nt] = t0[tb ^ in1];  // amplitude t + 4
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        float d[4] = {0.f, 0.f, 0.f, 0.f};
+        // k-step 0: real inputs, k-step 1: imaginary inputs
+        const float bv[2][2] = {{x0[nt].x, x1[nt].x}, {x0[nt].y, x1[nt].y}};
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+          uint32_t bh0, bl0, bh1, bl1;
+          split_tf32(bv[s][0], bh0, bl0);
+          split_tf32(bv[s][1], bh1, bl1);
+          mma_tf32(d, alo[s], bh0, bh1);
+          mma_tf32(d, ahi[s], bl0, bl1);
+          mma_tf32(d, ahi[s], bh0, bh1);
+        }
+        // d0, d1: real parts of amplitude g for groups 2t, 2t + 1; d2, d3: imaginary
+        const uint32_t tb = cb ^ T[nt];
+        t0[tb ^ out0] = make_float2(d[0], d[2]);
+        t0[tb ^ out1] = make_float2(d[1], d[3]);
+      }
+    }
+    __syncthreads();
+  }
+  store_tile<float2, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
+}
+
 // Rank over GF(2) of up to four 4-bit vectors.
 int gf2_rank(std::initializer_list<uint32_t> in) {
   uint32_t v[4];
@@ -692,7 +788,10 @@ qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool v
   if (qsv_status st = cuda_status(cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice,
                                                   s->stream), "dense plan upload"))
     return st;
-  void* kern = R == 3 ? (void*)k_dmma3<V> : (void*)k_dmma<V>;
+  // complex<float> three-bit passes: TF32 tensor cores with the three-term
+  // split unless FP64 is asked for (engine 2)
+  const bool tf32 = std::is_same<V, float2>::value && R == 3 && !(x.opts && x.opts->engine == 2);
+  void* kern = tf32 ? (void*)k_tf32x3 : (R == 3 ? (void*)k_dmma3<V> : (void*)k_dmma<V>);
   if (qsv_status st = cuda_status(cudaFuncSetAttribute(kern,
                                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                        200 * 1024), "dense stage shared-memory attribute"))

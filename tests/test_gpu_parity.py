@@ -82,9 +82,11 @@ def test_fused_matches_reference_within_tolerance(states, dtype):
     for cname, n, recs, op, off, x in circuit_cases(dtype):
         xn = x / np.linalg.norm(x)
         ref = oracle.apply(xn.astype(dtype), recs, op, off)
-        # engine 0 (tensor-core dense passes, complex states with tiles of
-        # >= 7 bits) and engine 1 (sparse register passes)
-        for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(tile_bits=4, low_bits=2),
+        # engine 0 (tensor-core dense passes for complex states with tiles of
+        # >= 7 bits: FP64 MMA, or TF32 three-term MMA for complex<float>),
+        # engine 1 (sparse register passes), engine 2 (FP64 MMA throughout)
+        for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=2),
+                     L.FuseOpts(tile_bits=4, low_bits=2),
                      L.FuseOpts(tile_bits=6, low_bits=1), L.FuseOpts(tile_bits=7, low_bits=2),
                      L.FuseOpts(tile_bits=12, low_bits=5, max_stage_gates=3),
                      L.FuseOpts(tile_bits=12, low_bits=5, max_stage_gates=3, engine=1)):
@@ -106,7 +108,7 @@ def test_random_mixed_large(states, dtype, n):
         ref = oracle.apply(x.copy(), recs, op)
         y = run_gpu(states, n, dtype, recs, op, 0, x)
         assert np.array_equal(y, ref)
-        for opts in (None, L.FuseOpts(engine=1)):
+        for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=2)):
             yf = run_gpu(states, n, dtype, recs, op, 0, x, fused=True, opts=opts)
             assert np.max(np.abs(yf - ref)) <= tol(dtype), (op, opts and opts.engine)
 
