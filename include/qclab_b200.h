@@ -157,7 +157,10 @@ typedef struct qsv_fuse_opts {
                         FP64 MMA for complex<double>, TF32 MMA with the
                         three-term split (FP32 accuracy) for complex<float>;
                         1 = sparse register passes on the CUDA cores;
-                        2 = FP64 MMA for complex<float> too                  */
+                        2 = FP64 MMA for complex<float> too;
+                        3 = complex<float> TF32 passes on tcgen05 with the
+                        state rows in tensor memory (tiles of 2^10 .. 2^13
+                        amplitudes; others as 0)                           */
   int reserved[2];
 } qsv_fuse_opts;
 

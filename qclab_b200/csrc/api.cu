@@ -4,6 +4,7 @@
 #include <cstring>
 #include <vector>
 #include "common.cuh"
+#include "fused.hpp"
 #include "internal.hpp"
 
 namespace qsv {
@@ -253,7 +254,8 @@ qsv_status qsv_download(qsv_state s, void* host, size_t bytes) {
   qsv_status st = cuda_status(cudaMemcpyAsync(host, s->d, bytes, cudaMemcpyDeviceToHost, s->stream),
                               "download cudaMemcpyAsync");
   if (st) return st;
-  return cuda_status(cudaStreamSynchronize(s->stream), "download synchronize");
+  if ((st = cuda_status(cudaStreamSynchronize(s->stream), "download synchronize"))) return st;
+  return tc_check_status();
 }
 
 qsv_status qsv_copy(qsv_state dst, qsv_state src) {
@@ -275,7 +277,8 @@ qsv_status qsv_set_basis(qsv_state s, uint64_t index) {
 
 qsv_status qsv_synchronize(qsv_state s) {
   if (qsv_status st = check_state(s)) return st;
-  return cuda_status(cudaStreamSynchronize(s->stream), "qsv_synchronize");
+  if (qsv_status st = cuda_status(cudaStreamSynchronize(s->stream), "qsv_synchronize")) return st;
+  return tc_check_status();
 }
 
 qsv_status qsv_apply(qsv_state s, const qsv_gate* gates, size_t nGates, char op, int offset) {

@@ -14,6 +14,7 @@
 // path for complex<double>, not bitwise: the planner reorders commuting
 // gates, which changes rounding).
 #include <algorithm>
+#include <atomic>
 #include <array>
 #include <complex>
 #include <initializer_list>
@@ -23,10 +24,12 @@
 #include <vector>
 #include "fused.hpp"
 #include "stage_exec.cuh"
+#include "tcgen05.cuh"
 
 namespace qsv {
 
 static thread_local std::vector<float> g_stage_ms;
+static std::atomic<bool> g_tc_used{false};  // a tcgen05 sweep was launched
 
 namespace fx {
 
@@ -640,6 +643,170 @@ __global__ void __launch_bounds__(256, 2) k_tf32x3(float2* __restrict__ v0, Dmma
   store_tile<float2, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
 }
 
+// ---- complex<float> passes on tcgen05 (kind::tf32), state rows in TMEM -----
+// A pass on three tile bits applies one 8x8 complex U to every group of 8
+// amplitudes.  As a GEMM, D[g][n] = sum_k X[g][k] W[k][n] with X[g] the row
+// (Re x_0..7, Im x_0..7) of group g and the real 16x16 W
+//   W[j][i] = Re U[i][j], W[8+j][i] = -Im U[i][j],
+//   W[j][8+i] = Im U[i][j], W[8+j][8+i] = Re U[i][j].
+// 128 groups form one M = 128 tile.  Each thread gathers its group from the
+// shared-memory state tile, splits the row into X_hi + X_lo (tc::tf32_split)
+// and stores the two halves to tensor memory; one thread per warpgroup then
+// issues
+//   D[:, 0:32]  = X_hi [W_hi | W_lo]     (N = 32, two K-steps of 8)
+//   D[:, 0:16] += X_lo W_hi              (N = 16, two K-steps)
+// and the output row is D[:, n] + D[:, 16 + n] (the X_lo W_lo term, about
+// 2^-22 relative, is dropped).  An MMA costs about the same for N = 16 and
+// N = 32 (12.9 and 13.0 ns per SM in a probe), so the W_lo product rides in
+// the upper half of the first pair.  Each warpgroup alternates two
+// tensor-memory slots (A_hi 16 | A_lo 16 | D 32 columns).  Per slot, one
+// mbarrier counts the 128 threads' stores of A (only the issuing thread
+// waits on it) and one receives the MMAs' commit; so a warp gathers the next
+// M tile while the tensor cores work on the previous one.  W, as tf32 hi/lo
+// halves, sits in shared memory in the K-major no-swizzle layout (8-row x
+// 16-byte core matrices; 512 bytes between K chunks, 128 bytes between
+// 8-row groups of N), double-buffered across passes; each thread builds one
+// entry per pass from a U element it loaded a pass earlier.
+constexpr uint32_t kTcCols = 256;        // tensor-memory columns per CTA
+constexpr int kTcWaitLimit = 2000;       // suspended polls (up to 1 ms each)
+constexpr size_t kTcMinSmem = 80 * 1024; // at most two CTAs (2 x 256 columns) per SM
+__device__ unsigned g_tc_status;         // non-zero: a tensor-core wait gave up
+
+// Entry e = threadIdx.x (k = e / 16, n = e % 16) of W: hi at column n, lo
+// at 16 + n, from u = U[n % 8][k % 8].
+__device__ __forceinline__ void tc_w_entry(float* img, double2 u) {
+  const int e = threadIdx.x, k = e >> 4, n = e & 15;
+  const double w = ((k < 8) == (n < 8)) ? u.x : (k < 8 ? u.y : -u.y);
+  const float hi = __uint_as_float(tc::tf32_round((float)w));
+  const float lo = __uint_as_float(tc::tf32_round((float)(w - (double)hi)));
+  const int kb = (k >> 2) * 128 + (k & 3) + (n & 7) * 4;
+  img[kb + (n >> 3) * 32] = hi;
+  img[kb + ((n + 16) >> 3) * 32] = lo;
+}
+__device__ __forceinline__ int tc_u_index() {  // U[i][j] at j * 8 + i
+  return ((threadIdx.x >> 4) & 7) * 8 + (threadIdx.x & 7);
+}
+
+__global__ void __launch_bounds__(256, 2) k_tc32(float2* __restrict__ v0, DmmaArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t size = 1u << a.ta.m;  // 2^10 .. 2^13 amplitudes
+  float2* t0 = reinterpret_cast<float2*>(smem_raw);
+  float* wimg = reinterpret_cast<float*>(smem_raw + size_t(size) * sizeof(float2));  // 2 x 2 KB
+  // bars[wg * 2 + s]: MMAs of slot s done; bars[4 + wg * 2 + s]: A of slot s stored
+  uint64_t* bars = reinterpret_cast<uint64_t*>(wimg + 1024);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 8);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
+  unsigned char* plan = reinterpret_cast<unsigned char*>(bars) + 128;
+  const PassDev* passes;
+  const POp* ops;
+  const double2* coefs_unused;
+  // tables and ops in shared memory; W is built from U in global memory
+  stage_plan<double2>(plan, a.passes, a.npasses, a.ops, a.nops, a.coefs, 0, &passes, &ops,
+                      &coefs_unused);
+  const int tid = threadIdx.x, warp = tid >> 5, wg = tid >> 7, r = tid & 127;
+  if (tid == 0) {
+    for (int b = 0; b < 4; ++b) tc::bar_init(bars + b, 1);
+    for (int b = 4; b < 8; ++b) tc::bar_init(bars + b, 128);
+    tc::bar_init_fence();
+    *abort_flag = 0;
+  }
+  if (warp == 0) tc::alloc(tslot, kTcCols);
+  const uint64_t base = tile_base(a.ta, blockIdx.x);
+  load_tile<float2, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
+  const int uix = tc_u_index();
+  double2 unext = make_double2(0.0, 0.0);
+  if (a.npasses > 0) tc_w_entry(wimg, a.coefs[a.ops[a.passes[0].op0].coef + uix]);
+  if (a.npasses > 1) unext = a.coefs[a.ops[a.passes[1].op0].coef + uix];
+  tc::fence_proxy_async();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tbase = *tslot;
+  const uint32_t lane_off = (uint32_t)((warp & 3) * 32) << 16;
+  const uint32_t nm = size >> 10;           // M tiles of 128 groups
+  const uint32_t jn = (nm + 1 - wg) / 2;    // this warpgroup's: i = 2 j + wg < nm
+  const uint32_t id32 = tc::idesc_tf32(128, 32), id16 = tc::idesc_tf32(128, 16);
+  uint64_t* done = bars + wg * 2;
+  uint64_t* stored = bars + 4 + wg * 2;
+  uint32_t uses = 0;  // bit s: parity of the next completion of slot s's barriers
+  for (int pi = 0; pi < a.npasses; ++pi) {
+    const uint16_t* T = passes[pi].off;
+    if (pi + 1 < a.npasses) tc_w_entry(wimg + ((pi + 1) & 1) * 512, unext);
+    if (pi + 2 < a.npasses) unext = a.coefs[ops[passes[pi + 2].op0].coef + uix];
+    const uint32_t wsm = tc::smem_addr(wimg + (pi & 1) * 512);
+    uint32_t ao[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) ao[j] = T[j];
+    uint32_t gr = 0;
+#pragma unroll
+    for (int b = 0; b < 7; ++b)
+      if ((r >> b) & 1) gr ^= T[8 + b];
+    uint32_t prev = 0;
+    for (uint32_t j = 0; j <= jn; ++j) {
+      uint32_t gb = 0;
+      if (j < jn) {
+        const uint32_t s = j & 1, i = 2 * j + wg;
+        gb = gr;
+        for (int b = 0; (i >> b) != 0u; ++b)
+          if ((i >> b) & 1u) gb ^= T[15 + b];
+        const uint32_t col = wg * 128 + s * 64;
+        uint32_t hi[16], lo[16];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const float2 x = t0[gb ^ ao[k]];
+          tc::tf32_split(x.x, hi[k], lo[k]);
+          tc::tf32_split(x.y, hi[8 + k], lo[8 + k]);
+        }
+        tc::st_32x32b_x16(tbase + lane_off + col, hi);
+        tc::st_32x32b_x16(tbase + lane_off + col + 16, lo);
+        tc::wait_st();
+        tc::fence_before();
+        tc::bar_arrive(stored + s);
+        if (r == 0) {
+          if (tc::bar_wait(stored + s, (uses >> s) & 1u, abort_flag, kTcWaitLimit)) {
+            tc::fence_after();
+            const uint32_t ta = tbase + col, td = tbase + col + 32;
+            const uint64_t b0 = tc::sdesc_kmajor(wsm, 512, 128);
+            const uint64_t b1 = tc::sdesc_kmajor(wsm + 1024, 512, 128);
+            tc::mma_tf32_ts(td, ta, b0, id32, 0);
+            tc::mma_tf32_ts(td, ta + 8, b1, id32, 1);
+            tc::mma_tf32_ts(td, ta + 16, b0, id16, 1);
+            tc::mma_tf32_ts(td, ta + 24, b1, id16, 1);
+            tc::commit(done + s);
+          } else {
+            *abort_flag = 1;
+            atomicOr(&g_tc_status, 1u);
+          }
+        }
+      }
+      if (j > 0) {  // finish M tile j - 1: wait for its MMAs, read D, scatter
+        const uint32_t s = (j - 1) & 1;
+        if (!tc::bar_wait(done + s, (uses >> s) & 1u, abort_flag, kTcWaitLimit)) {
+          *abort_flag = 1;
+          atomicOr(&g_tc_status, 1u);
+        }
+        uses ^= 1u << s;
+        __syncwarp();
+        tc::fence_after();
+        float d[32];
+        tc::ld_32x32b_x32(tbase + lane_off + wg * 128 + s * 64 + 32, d);
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          t0[prev ^ ao[k]] = make_float2(d[k] + d[16 + k], d[8 + k] + d[24 + k]);
+      }
+      prev = gb;
+    }
+    tc::fence_proxy_async();  // the next pass's W
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+  }
+  store_tile<float2, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0) tc::dealloc(tbase, kTcCols);
+}
+
 // Rank over GF(2) of up to four 4-bit vectors.
 int gf2_rank(std::initializer_list<uint32_t> in) {
   uint32_t v[4];
@@ -735,6 +902,45 @@ void dmma_tables_compute(PassDev* P, int R, int m, int epu) {
   for (int k = 0; k + 5 + nb < m && 12 + na + k < 32; ++k) P->off[12 + na + k] = ph(map(32u << k));
 }
 
+// Address tables of one tcgen05 pass (k_tc32) on tile bits p0 < p1 < p2 of
+// an m-bit complex<float> tile, in PassDev.off:
+//   off[j]      j < 8       amplitude part of amplitude j (pass bits)
+//   off[8 + k]  k < m - 3   group part of group bit k
+// Group bits 0..6 are the row of the M = 128 tile (bits 0..4 the lane), the
+// rest the M tile.  The four lowest are chosen, where the pass bits allow,
+// so that the banks a half-warp touches (8-byte elements: element index mod
+// 16) are all different.
+void tc_tables(PassDev* P, int m) {
+  const int pos[3] = {P->pos[0], P->pos[1], P->pos[2]};
+  std::vector<int> rest, sel;
+  for (int b = 0; b < m; ++b)
+    if (b != pos[0] && b != pos[1] && b != pos[2]) rest.push_back(b);
+  uint32_t basis[4] = {0, 0, 0, 0};  // reduced bank directions, by leading bit
+  auto independent_add = [&](uint32_t v) {
+    for (int bit = 3; bit >= 0; --bit) {
+      if (!((v >> bit) & 1u)) continue;
+      if (!basis[bit]) { basis[bit] = v; return true; }
+      v ^= basis[bit];
+    }
+    return false;
+  };
+  std::vector<bool> used(rest.size(), false);
+  for (size_t i = 0; i < rest.size() && sel.size() < 4; ++i)
+    if (independent_add((uint32_t)phys_host(1u << rest[i], 2) & 15u)) {
+      sel.push_back(rest[i]);
+      used[i] = true;
+    }
+  for (size_t i = 0; i < rest.size(); ++i)
+    if (!used[i]) sel.push_back(rest[i]);
+  for (int j = 0; j < 8; ++j) {
+    uint32_t e = 0;
+    for (int k = 0; k < 3; ++k)
+      if ((j >> k) & 1) e |= 1u << pos[k];
+    P->off[j] = (uint16_t)phys_host(e, 2);
+  }
+  for (int k = 0; k < m - 3; ++k) P->off[8 + k] = (uint16_t)phys_host(1u << sel[k], 2);
+}
+
 constexpr size_t kDmmaPlanMax = 96 * 1024;  // a tensor-core stage's plan bytes, at most
 
 // Tile bits of the tensor-core engine for an n-qubit complex sweep, or -1
@@ -765,12 +971,22 @@ qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool v
   if (qsv_status st = pack_plan<double2>(*x.items, n, m, low, R, max_gates, &plan, 1, kDmmaPlanMax))
     return st;
   if (plan.stages.empty()) return QSV_SUCCESS;
+  // complex<float> three-bit passes: TF32 with the three-term split, on
+  // mma.sync (default) or on tcgen05 with the state rows in tensor memory
+  // (engine 3, tiles of 2^10 .. 2^13 amplitudes); engine 2 keeps FP64 MMA
+  const int engine = x.opts ? x.opts->engine : 0;
+  const bool tf32 = std::is_same<V, float2>::value && R == 3 && engine != 2;
+  const bool tcg = tf32 && engine == 3 && m >= 10 && m <= 13;
   for (const PackedStage& ps : plan.stages)
     for (size_t pi = ps.pass0; pi < ps.pass0 + ps.npasses; ++pi) {
       PassDev& P = plan.passes[pi];
-      if (P.nops != 1 || plan.ops[ps.op0 + P.op0].shape != P_DENSE || ps.m < 5 + R)
+      if (P.nops != 1 || plan.ops[ps.op0 + P.op0].shape != P_DENSE || ps.m < 5 + R ||
+          (tcg && ps.m < 10))
         return QSV_ERROR_NOT_SUPPORTED;
-      dmma_tables(&P, R, ps.m, Units<V>::per);
+      if (tcg)
+        tc_tables(&P, ps.m);
+      else
+        dmma_tables(&P, R, ps.m, Units<V>::per);
     }
   auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
   const size_t pass_bytes = plan.passes.size() * sizeof(PassDev);
@@ -788,10 +1004,9 @@ qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool v
   if (qsv_status st = cuda_status(cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice,
                                                   s->stream), "dense plan upload"))
     return st;
-  // complex<float> three-bit passes: TF32 tensor cores with the three-term
-  // split unless FP64 is asked for (engine 2)
-  const bool tf32 = std::is_same<V, float2>::value && R == 3 && !(x.opts && x.opts->engine == 2);
-  void* kern = tf32 ? (void*)k_tf32x3 : (R == 3 ? (void*)k_dmma3<V> : (void*)k_dmma<V>);
+  void* kern = tcg ? (void*)k_tc32
+                   : (tf32 ? (void*)k_tf32x3 : (R == 3 ? (void*)k_dmma3<V> : (void*)k_dmma<V>));
+  if (tcg) g_tc_used = true;
   if (qsv_status st = cuda_status(cudaFuncSetAttribute(kern,
                                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                        200 * 1024), "dense stage shared-memory attribute"))
@@ -823,7 +1038,10 @@ qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool v
     a.coefs = reinterpret_cast<const double2*>(dev + coef_off) + ps.coef0;
     a.vec16 = vec16 ? 1 : 0;
     const size_t smem_stage =
-        (size_t(1) << ps.m) * sizeof(V) + plan_smem_bytes<double2>((int)ps.npasses, ps.nops, ps.ncoef);
+        tcg ? std::max(kTcMinSmem, (size_t(1) << ps.m) * sizeof(V) + 4096 + 128 +
+                                       plan_smem_bytes<double2>((int)ps.npasses, ps.nops, 0))
+            : (size_t(1) << ps.m) * sizeof(V) +
+                  plan_smem_bytes<double2>((int)ps.npasses, ps.nops, ps.ncoef);
     void* args[] = {&p0, &a};
     if (qsv_status st = cuda_status(cudaLaunchKernel(kern, dim3((unsigned)ntiles),
                                                      dim3(256), args, smem_stage, s->stream),
@@ -984,6 +1202,18 @@ int effective_tile_bits(size_t eb, int nv, int n, const qsv_fuse_opts* opts) {
   return m;
 }
 int default_low_bits(size_t eb) { return eb >= 16 ? 2 : 3; }
+
+qsv_status tc_check_status() {
+  if (!g_tc_used.load(std::memory_order_relaxed)) return QSV_SUCCESS;
+  unsigned v = 0;
+  if (qsv_status st = cuda_status(cudaMemcpyFromSymbol(&v, g_tc_status, sizeof(v)),
+                                  "tensor-core status read"))
+    return st;
+  if (!v) return QSV_SUCCESS;
+  const unsigned zero = 0;
+  cudaMemcpyToSymbol(g_tc_status, &zero, sizeof(zero));
+  return fail(QSV_ERROR_TIMEOUT, "a tensor-core sweep gave up waiting for its MMAs (results invalid)");
+}
 
 qsv_status execute_fused(const ExecArgs& x) {
   switch (x.s->dtype) {

@@ -28,6 +28,10 @@ int default_low_bits(size_t elem_bytes);
 // Plans the items into stages and runs them.
 qsv_status execute_fused(const ExecArgs& x);
 
+// QSV_ERROR_TIMEOUT once (and clears it) if a tcgen05 sweep's bounded wait
+// gave up since the last call; call after the stream has synchronised.
+qsv_status tc_check_status();
+
 // Tile bits the executor uses for nv vectors of an n-qubit state: the
 // requested (or default) size, at most 14 and n, and at most 256 threads of
 // 2^r amplitudes (times the groups a thread takes per pass).

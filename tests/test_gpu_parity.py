@@ -84,8 +84,10 @@ def test_fused_matches_reference_within_tolerance(states, dtype):
         ref = oracle.apply(xn.astype(dtype), recs, op, off)
         # engine 0 (tensor-core dense passes for complex states with tiles of
         # >= 7 bits: FP64 MMA, or TF32 three-term MMA for complex<float>),
-        # engine 1 (sparse register passes), engine 2 (FP64 MMA throughout)
-        for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=2),
+        # engine 1 (sparse register passes), engine 2 (FP64 MMA throughout),
+        # engine 3 (complex<float> TF32 on tcgen05 for tiles of >= 10 bits)
+        for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=2), L.FuseOpts(engine=3),
+                     L.FuseOpts(tile_bits=10, low_bits=3, engine=3),
                      L.FuseOpts(tile_bits=4, low_bits=2),
                      L.FuseOpts(tile_bits=6, low_bits=1), L.FuseOpts(tile_bits=7, low_bits=2),
                      L.FuseOpts(tile_bits=12, low_bits=5, max_stage_gates=3),
@@ -108,9 +110,29 @@ def test_random_mixed_large(states, dtype, n):
         ref = oracle.apply(x.copy(), recs, op)
         y = run_gpu(states, n, dtype, recs, op, 0, x)
         assert np.array_equal(y, ref)
-        for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=2)):
+        for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=2), L.FuseOpts(engine=3)):
             yf = run_gpu(states, n, dtype, recs, op, 0, x, fused=True, opts=opts)
             assert np.max(np.abs(yf - ref)) <= tol(dtype), (op, opts and opts.engine)
+
+
+@pytest.mark.parametrize("tile_bits", [10, 11, 12, 13])
+def test_tcgen05_tiles(states, tile_bits):
+    """complex<float> sweeps on tcgen05 (engine 3): tiles of 1 to 8 M = 128
+    group tiles (one or both warpgroups busy), against the oracle."""
+    n = 15
+    dtype = np.complex64
+    rng = np.random.default_rng(tile_bits)
+    recs = W.random_mixed(n, 150, seed=tile_bits).gate_records(dtype)
+    x = (rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)).astype(dtype)
+    x /= np.linalg.norm(x)
+    ref = oracle.apply(x.copy(), recs, "N")
+    opts = L.FuseOpts(tile_bits=tile_bits, low_bits=3, engine=3)
+    before = launch_count()
+    y = run_gpu(states, n, dtype, recs, "N", 0, x, fused=True, opts=opts)
+    assert launch_count() > before
+    assert np.max(np.abs(y - ref)) <= tol(dtype)
+    # the three-term split keeps FP32-level accuracy: no visible norm drift
+    assert abs(np.vdot(y.astype(np.complex128), y.astype(np.complex128)).real - 1.0) < 1e-5
 
 
 def test_qft20_config(states):
