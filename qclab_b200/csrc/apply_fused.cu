@@ -112,7 +112,8 @@ template <> float dense_coef<float>(cplxd z) { return (float)z.real(); }
 
 template <typename V>
 qsv_status pack_plan(const std::vector<Lowered>& gates, int n, int m, int low, int r,
-                     int max_gates, PackedPlan<V>* out, int dense_min, size_t plan_cap) {
+                     int max_gates, PackedPlan<V>* out, int dense_min, size_t plan_cap,
+                     bool search_passes) {
   const int min_ops = dense_min >= 0 ? dense_min : QSV_DENSE_MIN_OPS;
   constexpr bool cplx = Elem<V>::cplx;
   std::vector<Stage> stages =
@@ -141,7 +142,7 @@ qsv_status pack_plan(const std::vector<Lowered>& gates, int n, int m, int low, i
     };
     std::vector<uint32_t> op_bits;
     for (int gi : stg.gates) op_bits.push_back(local_mask(gate_bits(gates[gi])));
-    std::vector<Pass> pl = plan_passes(op_bits, stg.m, r);
+    std::vector<Pass> pl = plan_passes(op_bits, stg.m, r, search_passes);
     // Phase 1: every pass packed sparse into its own buffers (op.coef
     // relative to the pass), with its coefficients also kept in FP64.
     struct PassBuf {
@@ -301,10 +302,10 @@ qsv_status pack_plan(const std::vector<Lowered>& gates, int n, int m, int low, i
   return QSV_SUCCESS;
 }
 
-template qsv_status pack_plan<double2>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<double2>*, int, size_t);
-template qsv_status pack_plan<float2>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<float2>*, int, size_t);
-template qsv_status pack_plan<double>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<double>*, int, size_t);
-template qsv_status pack_plan<float>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<float>*, int, size_t);
+template qsv_status pack_plan<double2>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<double2>*, int, size_t, bool);
+template qsv_status pack_plan<float2>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<float2>*, int, size_t, bool);
+template qsv_status pack_plan<double>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<double>*, int, size_t, bool);
+template qsv_status pack_plan<float>(const std::vector<Lowered>&, int, int, int, int, int, PackedPlan<float>*, int, size_t, bool);
 
 }  // namespace fx
 
@@ -968,7 +969,8 @@ qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool v
   PackedPlan<double2> plan;
   // plans sized per launch: a few KB typically, at most kDmmaPlanMax
   if ((size_t(1) << m) * sizeof(V) + kDmmaPlanMax > 200 * 1024) return QSV_ERROR_NOT_SUPPORTED;
-  if (qsv_status st = pack_plan<double2>(*x.items, n, m, low, R, max_gates, &plan, 1, kDmmaPlanMax))
+  if (qsv_status st = pack_plan<double2>(*x.items, n, m, low, R, max_gates, &plan, 1, kDmmaPlanMax,
+                                         QSV_DENSE_SEARCH != 0))
     return st;
   if (plan.stages.empty()) return QSV_SUCCESS;
   // complex<float> three-bit passes: TF32 with the three-term split, on
@@ -1258,7 +1260,7 @@ qsv_status plan_counts(const std::vector<Lowered>& low, int n, const qsv_fuse_op
     const int max_gates = (opts && opts->max_stage_gates > 0) ? opts->max_stage_gates : 256;
     fx::PackedPlan<double2> plan;
     if (qsv_status st = fx::pack_plan<double2>(low, n, md, lowb, dmma_pass_bits(md), max_gates, &plan, 1,
-                                               kDmmaPlanMax))
+                                               kDmmaPlanMax, QSV_DENSE_SEARCH != 0))
       return st;
     for (const fx::PackedStage& ps : plan.stages) {
       ops->push_back(ps.nops);

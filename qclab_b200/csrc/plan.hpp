@@ -80,6 +80,13 @@ struct Pass {
 // register passes of at most r bits, with the same blocking rule as
 // plan_stages, so each pass is a valid reordering of commuting ops.  Every
 // pass is padded to exactly r bits (the lowest unused local bits; m >= r).
-std::vector<Pass> plan_passes(const std::vector<uint32_t>& op_bits, int m, int r);
+// search = false: each pass takes ops in order while their bits fit in r
+// (greedy).  search = true (passes multiplied out into dense matrices, whose
+// cost does not depend on how many ops they hold): each pass's r bits are
+// the set, among the greedy one and every r-bit set holding the first
+// remaining op, after which the greedy planner needs the fewest passes for
+// the rest of the stage (ties keep the greedy set).
+std::vector<Pass> plan_passes(const std::vector<uint32_t>& op_bits, int m, int r,
+                              bool search = false);
 
 }  // namespace qsv

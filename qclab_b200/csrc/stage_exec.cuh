@@ -58,6 +58,11 @@
 #ifndef QSV_DMMA_BITS
 #define QSV_DMMA_BITS 3
 #endif
+// Tensor-core plans: each pass's bits chosen to absorb the most ops (1) or
+// greedily in circuit order (0).
+#ifndef QSV_DENSE_SEARCH
+#define QSV_DENSE_SEARCH 1
+#endif
 #ifndef QSV_TURN_BITS_C128  // log2 register groups per thread and pass (complex<double>)
 #define QSV_TURN_BITS_C128 0
 #endif
@@ -740,7 +745,7 @@ struct PackedPlan {
 template <typename V>
 qsv_status pack_plan(const std::vector<Lowered>& gates, int n, int m, int low, int r,
                      int max_gates, PackedPlan<V>* out, int dense_min = -1,
-                     size_t plan_cap = kPlanSmemMax);
+                     size_t plan_cap = kPlanSmemMax, bool search_passes = false);
 
 }  // namespace fx
 }  // namespace qsv
