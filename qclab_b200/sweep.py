@@ -1,15 +1,25 @@
 """Times fused sweeps from the command line.
 
     python -m qclab_b200.sweep --qubits 26 --depth 40 --dtype c64 --engine 3
+    python -m qclab_b200.sweep --workload adjoint --qubits 22 --depth 12
+    python -m qclab_b200.sweep --workload batch --circuits 512
 
-Runs a seeded random brick circuit (``workloads.brick``) through
+brick (default): a seeded random brick circuit (``workloads.brick``) through
 ``qsv_apply_fused`` on the current GPU, ``--repeat`` times after one warm-up
-sweep, and prints one JSON line: gates, stages and tensor-core passes of the
-plan (``qsv_plan_passes``), the wall time of each sweep (host planning
+sweep; prints one JSON line with the gates, stages and tensor-core passes of
+the plan (``qsv_plan_passes``), the wall time of each sweep (host planning
 included, stream synchronised) and gates/s.  ``--engine`` is
 ``qsv_fuse_opts.engine``: 0 default (FP64 MMA for complex<double>, mma.sync
 TF32 for complex<float>), 1 sparse register passes, 2 FP64 MMA for both,
 3 tcgen05 TF32 for complex<float>.
+
+adjoint: energy and full gradient (``qsv_adjoint_gradient``) of the
+hardware-efficient ansatz ``workloads.hea(qubits, depth)`` for
+H = sum Z_i Z_i+1 + 0.5 sum X_i; prints the time per gradient.
+
+batch: ``--circuits`` ansatz circuits of 8..18 qubits and 4..16 layers in one
+persistent launch (``qsv_batch_run``, default tile shape); prints the time
+per batch.
 """
 from __future__ import annotations
 
@@ -36,7 +46,13 @@ def main(argv=None) -> dict:
     p.add_argument("--engine", type=int, default=0)
     p.add_argument("--tile-bits", type=int, default=0)
     p.add_argument("--repeat", type=int, default=2)
+    p.add_argument("--workload", choices=["brick", "adjoint", "batch"], default="brick")
+    p.add_argument("--circuits", type=int, default=512)
     a = p.parse_args(argv)
+    if a.workload == "adjoint":
+        return _adjoint(a)
+    if a.workload == "batch":
+        return _batch(a)
     dt, code = DTYPES[a.dtype]
     recs = W.brick(a.qubits, a.depth, seed=a.seed).gate_records(dt)
     opts = L.FuseOpts(engine=a.engine, tile_bits=a.tile_bits)
@@ -60,6 +76,56 @@ def main(argv=None) -> dict:
             ms.append((time.perf_counter() - t) * 1e3)
     out["ms"] = [round(v, 3) for v in ms]
     out["gates_per_s"] = cnt / (min(ms) / 1e3) if ms else None
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def _timed(fn, repeat):
+    fn()
+    ms = []
+    for _ in range(repeat):
+        t = time.perf_counter()
+        fn()
+        ms.append((time.perf_counter() - t) * 1e3)
+    return [round(v, 3) for v in ms]
+
+
+def _adjoint(a) -> dict:
+    from .gradients import adjoint_gradient
+    from .observable import ising
+    dt, _ = DTYPES[a.dtype]
+    recs = W.hea(a.qubits, a.depth, seed=a.seed).gate_records(dt, number_params=True)
+    nparams = int(recs["param"].max()) + 1
+    H = ising(a.qubits)
+    out = {"workload": "adjoint", "qubits": a.qubits, "layers": a.depth, "dtype": a.dtype,
+           "gates": len(recs), "params": nparams}
+    with StateVector(a.qubits, dt) as s:
+        res = {}
+
+        def run():
+            res["e"], res["g"] = adjoint_gradient(s, recs, H, nparams)
+        out["ms"] = _timed(run, a.repeat)
+        out["energy"] = res["e"]
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def _batch(a) -> dict:
+    from .batch import Batch
+    from .observable import ising
+    dt, _ = DTYPES[a.dtype]
+    rng = np.random.default_rng(a.seed)
+    ns = rng.integers(8, 19, size=a.circuits)
+    ls = rng.integers(4, 17, size=a.circuits)
+    circs = [W.hea(int(n), int(l), seed=a.seed * 100003 + i) for i, (n, l) in enumerate(zip(ns, ls))]
+    obs = [ising(int(n)) for n in ns]
+    out = {"workload": "batch", "circuits": a.circuits, "dtype": a.dtype,
+           "gates": int(sum(len(c.gate_records(dt)) for c in circs))}
+    with Batch(circs, obs, dt) as b:
+        def run():
+            b.run()
+            b.results()
+        out["ms"] = _timed(run, a.repeat)
     print(json.dumps(out), flush=True)
     return out
 

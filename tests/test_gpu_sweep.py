@@ -1,0 +1,24 @@
+"""The sweep timing command (python -m qclab_b200.sweep) on every engine."""
+import pytest
+
+from qclab_b200 import sweep
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("dtype,engine", [("c128", 0), ("c128", 1), ("c64", 0), ("c64", 2),
+                                          ("c64", 3)])
+def test_sweep_command(cuda, dtype, engine):
+    out = sweep.main(["--qubits", "14", "--depth", "6", "--dtype", dtype, "--engine",
+                      str(engine), "--repeat", "1"])
+    assert out["gates"] == 14 * 6 + sum(len(range(l % 2, 13, 2)) for l in range(6))
+    assert out["stages"] >= 1 and out["passes"] >= out["stages"]
+    assert len(out["ms"]) == 1 and out["gates_per_s"] > 0
+
+
+def test_sweep_adjoint_and_batch(cuda):
+    out = sweep.main(["--workload", "adjoint", "--qubits", "10", "--depth", "3", "--repeat", "1"])
+    assert out["params"] == 10 * 2 * 3 and len(out["ms"]) == 1
+    assert -20.0 < out["energy"] < 20.0
+    out = sweep.main(["--workload", "batch", "--circuits", "16", "--dtype", "c64", "--repeat", "1"])
+    assert out["circuits"] == 16 and out["gates"] > 0 and len(out["ms"]) == 1
