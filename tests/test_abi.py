@@ -67,6 +67,22 @@ def test_planner_covers_every_gate_once():
         assert 0 < stages.value <= passes.value
 
 
+def test_tensor_plans_need_no_more_passes_than_greedy():
+    """The tensor-core engine picks each pass's bits by a greedy rollout, which
+    never needs more passes than the plain in-order greedy planner.  The
+    bounds are that planner's pass counts for these circuits."""
+    lib = L.load()
+    cases = [(W.brick(30, 200, seed=3), 1992), (W.qft(30), 251),
+             (W.random_mixed(24, 2000, seed=1), 565)]
+    for c, greedy in cases:
+        recs = c.gate_records(np.complex128)
+        stages, passes, ops = C.c_int(), C.c_int(), C.c_int()
+        assert lib.qsv_plan_passes(c.nbQubits(), L.C128, C.c_void_p(recs.ctypes.data), len(recs),
+                                   b"N", 0, None, C.byref(stages), C.byref(passes),
+                                   C.byref(ops)) == 0
+        assert 0 < passes.value <= greedy
+
+
 def test_planner_errors_are_status_codes():
     c = W.brick(6, 2, seed=1)
     recs = c.gate_records(np.complex128)
