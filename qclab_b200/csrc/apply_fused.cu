@@ -959,6 +959,32 @@ int dmma_tile_bits(int n, const qsv_fuse_opts* opts) {
 
 int dmma_pass_bits(int m) { return (QSV_DMMA_BITS == 3 && m >= 8) ? 3 : 2; }
 
+// The tensor-core engine's plan.  A dense pass costs the same whatever it
+// holds, and the pass count depends strongly on which low bits every tile
+// keeps (brick circuits: 1982 passes with 2 low bits, 1782 with 3, for 30
+// qubits and 12 tile bits); so when the caller leaves low_bits unset, the
+// default and one more contiguous low bit are both planned and the plan
+// with fewer passes (then fewer stages) is kept.
+qsv_status pack_dense_plan(const std::vector<Lowered>& items, int n, int m, int low,
+                           bool low_fixed, int R, int max_gates, PackedPlan<double2>* plan,
+                           int* low_used) {
+  *low_used = low;
+  if (qsv_status st = pack_plan<double2>(items, n, m, low, R, max_gates, plan, 1, kDmmaPlanMax,
+                                         QSV_DENSE_SEARCH != 0))
+    return st;
+  if (low_fixed || low + 1 > m || QSV_DENSE_LOW_SEARCH == 0) return QSV_SUCCESS;
+  PackedPlan<double2> alt;
+  if (pack_plan<double2>(items, n, m, low + 1, R, max_gates, &alt, 1, kDmmaPlanMax,
+                         QSV_DENSE_SEARCH != 0) != QSV_SUCCESS)
+    return QSV_SUCCESS;  // keep the first plan
+  if (alt.passes.size() < plan->passes.size() ||
+      (alt.passes.size() == plan->passes.size() && alt.stages.size() < plan->stages.size())) {
+    *plan = std::move(alt);
+    *low_used = low + 1;
+  }
+  return QSV_SUCCESS;
+}
+
 // Single-vector sweep of a complex state on the tensor-core engine; returns
 // QSV_ERROR_NOT_SUPPORTED (nothing launched) when the plan does not fit it.
 template <typename V>
@@ -969,8 +995,8 @@ qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool v
   PackedPlan<double2> plan;
   // plans sized per launch: a few KB typically, at most kDmmaPlanMax
   if ((size_t(1) << m) * sizeof(V) + kDmmaPlanMax > 200 * 1024) return QSV_ERROR_NOT_SUPPORTED;
-  if (qsv_status st = pack_plan<double2>(*x.items, n, m, low, R, max_gates, &plan, 1, kDmmaPlanMax,
-                                         QSV_DENSE_SEARCH != 0))
+  const bool low_fixed = x.opts && x.opts->low_bits > 0;
+  if (qsv_status st = pack_dense_plan(*x.items, n, m, low, low_fixed, R, max_gates, &plan, &low))
     return st;
   if (plan.stages.empty()) return QSV_SUCCESS;
   // complex<float> three-bit passes: TF32 with the three-term split, on
@@ -1259,8 +1285,9 @@ qsv_status plan_counts(const std::vector<Lowered>& low, int n, const qsv_fuse_op
     const int lowb = std::min((opts && opts->low_bits > 0) ? opts->low_bits : default_low_bits(sizeof(V)), md);
     const int max_gates = (opts && opts->max_stage_gates > 0) ? opts->max_stage_gates : 256;
     fx::PackedPlan<double2> plan;
-    if (qsv_status st = fx::pack_plan<double2>(low, n, md, lowb, dmma_pass_bits(md), max_gates, &plan, 1,
-                                               kDmmaPlanMax, QSV_DENSE_SEARCH != 0))
+    int low_used = lowb;
+    if (qsv_status st = pack_dense_plan(low, n, md, lowb, opts && opts->low_bits > 0,
+                                            dmma_pass_bits(md), max_gates, &plan, &low_used))
       return st;
     for (const fx::PackedStage& ps : plan.stages) {
       ops->push_back(ps.nops);

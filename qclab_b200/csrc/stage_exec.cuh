@@ -63,6 +63,11 @@
 #ifndef QSV_DENSE_SEARCH
 #define QSV_DENSE_SEARCH 1
 #endif
+// Tensor-core plans with unset low_bits: also plan one more low bit and keep
+// the plan with fewer passes (1), or keep the default (0).
+#ifndef QSV_DENSE_LOW_SEARCH
+#define QSV_DENSE_LOW_SEARCH 1
+#endif
 #ifndef QSV_TURN_BITS_C128  // log2 register groups per thread and pass (complex<double>)
 #define QSV_TURN_BITS_C128 0
 #endif
