@@ -153,20 +153,27 @@ typedef struct qsv_fuse_opts {
   int profile;       /* 1: time every stage with CUDA events (see below)   */
   int engine;        /* complex single-vector sweeps: 0 (default) = every
                         register pass of 3 tile bits multiplied out into an
-                        8x8 complex matrix and applied on the tensor cores --
-                        FP64 MMA for complex<double>, TF32 MMA with the
-                        three-term split (FP32 accuracy) for complex<float>;
+                        8x8 complex matrix in FP64 and applied on the FP64
+                        tensor cores (mma.sync f64), complex<float> states
+                        rounded once per pass;
                         1 = sparse register passes on the CUDA cores;
-                        2 = FP64 MMA for complex<float> too;
-                        3 = complex<float> TF32 passes on tcgen05 with the
-                        state rows in tensor memory (tiles of 2^10 .. 2^13
-                        amplitudes; others as 0)                           */
+                        2 = same as 0;
+                        3 = complex<float>: TF32 three-term split on tcgen05
+                        with the state rows in tensor memory (tiles of
+                        2^10 .. 2^13 amplitudes, else as 4);
+                        4 = complex<float>: TF32 three-term split on
+                        mma.sync.  The TF32 engines are faster but their
+                        FP32 accumulation truncates: the norm shrinks by
+                        about 1e-7 per pass.                               */
   int reserved[2];
 } qsv_fuse_opts;
 
 /* Fused path: the gate list is planned into stages; each stage streams the
  * state through shared memory once and applies all of its gates there.
- * Within 1e-12 (complex<double>) of qsv_apply, not bitwise.               */
+ * Within 1e-12 (complex<double>) of qsv_apply, not bitwise.  Gates are
+ * lowered and multiplied out in FP64 for every element type, so for a
+ * complex<float> state the fused result is closer to the exact circuit than
+ * the reference's float arithmetic (qsv_apply reproduces the latter).     */
 qsv_status qsv_apply_fused(qsv_state state, const qsv_gate* gates,
                            size_t nGates, char op, int offset,
                            const qsv_fuse_opts* opts);

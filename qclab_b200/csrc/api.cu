@@ -113,12 +113,12 @@ qsv_status check_state(qsv_state s) {
 
 qsv_status lower_for_state(const qsv_state_s* s, const qsv_gate* gates,
                            size_t count, char op, int offset,
-                           std::vector<Lowered>* out) {
+                           std::vector<Lowered>* out, bool fp64) {
   if (!valid_op(op)) return fail(QSV_ERROR_INVALID_VALUE, "op must be 'N', 'T' or 'C' (got %d)", (int)op);
   if (count && !gates) return fail(QSV_ERROR_INVALID_VALUE, "null gate list");
   out->assign(count, Lowered());
   size_t bad = 0;
-  qsv_status st = dtype_double(s->dtype)
+  qsv_status st = (fp64 || dtype_double(s->dtype))
       ? lower_list<double>(gates, count, op, offset, s->n, dtype_real(s->dtype), out->data(), &bad)
       : lower_list<float>(gates, count, op, offset, s->n, dtype_real(s->dtype), out->data(), &bad);
   if (st != QSV_SUCCESS) {
@@ -294,7 +294,10 @@ qsv_status qsv_apply_fused(qsv_state s, const qsv_gate* gates, size_t nGates, ch
                            int offset, const qsv_fuse_opts* opts) {
   if (qsv_status st = check_state(s)) return st;
   std::vector<Lowered> low;
-  if (qsv_status st = lower_for_state(s, gates, nGates, op, offset, &low)) return st;
+  // the fused sweeps multiply gates into dense matrices in FP64: lower every
+  // gate in double (a complex<float> state's gates too), not in the state's
+  // precision as the reference-exact path does
+  if (qsv_status st = lower_for_state(s, gates, nGates, op, offset, &low, true)) return st;
   return run_fused(s, low, opts);
 }
 

@@ -999,12 +999,16 @@ qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool v
   if (qsv_status st = pack_dense_plan(*x.items, n, m, low, low_fixed, R, max_gates, &plan, &low))
     return st;
   if (plan.stages.empty()) return QSV_SUCCESS;
-  // complex<float> three-bit passes: TF32 with the three-term split, on
-  // mma.sync (default) or on tcgen05 with the state rows in tensor memory
-  // (engine 3, tiles of 2^10 .. 2^13 amplitudes); engine 2 keeps FP64 MMA
+  // complex<float> three-bit passes run on FP64 MMA like complex<double>
+  // (rounded to nearest once per pass, so the norm does not drift); TF32
+  // with the three-term split is opt-in: on tcgen05 with the state rows in
+  // tensor memory (engine 3, tiles of 2^10 .. 2^13 amplitudes) or on
+  // mma.sync (engine 4, and engine 3 for smaller tiles).  Its FP32
+  // accumulation truncates, which shrinks the norm by ~1e-7 per pass.
   const int engine = x.opts ? x.opts->engine : 0;
-  const bool tf32 = std::is_same<V, float2>::value && R == 3 && engine != 2;
-  const bool tcg = tf32 && engine == 3 && m >= 10 && m <= 13;
+  const bool f32 = std::is_same<V, float2>::value && R == 3;
+  const bool tcg = f32 && engine == 3 && m >= 10 && m <= 13;
+  const bool tf32 = f32 && (engine == 4 || engine == 3);
   for (const PackedStage& ps : plan.stages)
     for (size_t pi = ps.pass0; pi < ps.pass0 + ps.npasses; ++pi) {
       PassDev& P = plan.passes[pi];
@@ -1317,7 +1321,7 @@ qsv_status plan_counts_any(int nbQubits, qsv_dtype dtype, const qsv_gate* gates,
   fake.n = nbQubits;
   fake.dtype = dtype;
   std::vector<Lowered> low;
-  if (qsv_status st = lower_for_state(&fake, gates, nGates, op, offset, &low)) return st;
+  if (qsv_status st = lower_for_state(&fake, gates, nGates, op, offset, &low, true)) return st;
   switch (dtype) {
     case QSV_C128: return plan_counts<double2>(low, nbQubits, opts, ops, passes);
     case QSV_C64:  return plan_counts<float2>(low, nbQubits, opts, ops, passes);

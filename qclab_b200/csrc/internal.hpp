@@ -47,9 +47,11 @@ inline uint64_t dim(int n) { return 1ull << n; }
 constexpr int kMaxQubits = 40;
 
 // Lowers a gate list for a state (dispatches on the state's real type).
+// fp64: lower in double whatever the state's precision (the fused sweeps);
+// otherwise in the state's real type, as the reference's templates do.
 qsv_status lower_for_state(const qsv_state_s* s, const qsv_gate* gates,
                            size_t count, char op, int offset,
-                           std::vector<Lowered>* out);
+                           std::vector<Lowered>* out, bool fp64 = false);
 
 // Grows the state's device scratch buffer to at least `bytes` (stream-ordered
 // with respect to earlier work on the state's stream).

@@ -9,9 +9,9 @@ brick (default): a seeded random brick circuit (``workloads.brick``) through
 sweep; prints one JSON line with the gates, stages and tensor-core passes of
 the plan (``qsv_plan_passes``), the wall time of each sweep (host planning
 included, stream synchronised) and gates/s.  ``--engine`` is
-``qsv_fuse_opts.engine``: 0 default (FP64 MMA for complex<double>, mma.sync
-TF32 for complex<float>), 1 sparse register passes, 2 FP64 MMA for both,
-3 tcgen05 TF32 for complex<float>.
+``qsv_fuse_opts.engine``: 0 default (FP64 MMA), 1 sparse register passes,
+2 as 0, 3 tcgen05 TF32 for complex<float>, 4 mma.sync TF32 for
+complex<float>.
 
 adjoint: energy and full gradient (``qsv_adjoint_gradient``) of the
 hardware-efficient ansatz ``workloads.hea(qubits, depth)`` for

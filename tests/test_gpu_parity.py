@@ -83,10 +83,11 @@ def test_fused_matches_reference_within_tolerance(states, dtype):
         xn = x / np.linalg.norm(x)
         ref = oracle.apply(xn.astype(dtype), recs, op, off)
         # engine 0 (tensor-core dense passes for complex states with tiles of
-        # >= 7 bits: FP64 MMA, or TF32 three-term MMA for complex<float>),
-        # engine 1 (sparse register passes), engine 2 (FP64 MMA throughout),
-        # engine 3 (complex<float> TF32 on tcgen05 for tiles of >= 10 bits)
+        # >= 7 bits, FP64 MMA), engine 1 (sparse register passes), engine 2
+        # (as 0), engine 3 (complex<float> TF32 on tcgen05 for tiles of >= 10
+        # bits), engine 4 (complex<float> TF32 on mma.sync)
         for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=2), L.FuseOpts(engine=3),
+                     L.FuseOpts(engine=4),
                      L.FuseOpts(tile_bits=10, low_bits=3, engine=3),
                      L.FuseOpts(tile_bits=4, low_bits=2),
                      L.FuseOpts(tile_bits=6, low_bits=1), L.FuseOpts(tile_bits=7, low_bits=2),
@@ -110,7 +111,8 @@ def test_random_mixed_large(states, dtype, n):
         ref = oracle.apply(x.copy(), recs, op)
         y = run_gpu(states, n, dtype, recs, op, 0, x)
         assert np.array_equal(y, ref)
-        for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=2), L.FuseOpts(engine=3)):
+        for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=2), L.FuseOpts(engine=3),
+                     L.FuseOpts(engine=4)):
             yf = run_gpu(states, n, dtype, recs, op, 0, x, fused=True, opts=opts)
             assert np.max(np.abs(yf - ref)) <= tol(dtype), (op, opts and opts.engine)
 
@@ -133,6 +135,26 @@ def test_tcgen05_tiles(states, tile_bits):
     assert np.max(np.abs(y - ref)) <= tol(dtype)
     # the three-term split keeps FP32-level accuracy: no visible norm drift
     assert abs(np.vdot(y.astype(np.complex128), y.astype(np.complex128)).real - 1.0) < 1e-5
+
+
+def test_complex_float_fused_keeps_the_norm(states):
+    """The default fused path multiplies gates out in FP64 and rounds a
+    complex<float> state once per pass to nearest: over a deep circuit the
+    norm stays put and the state stays within FP32 accuracy of the
+    complex<double> one (1 - |<psi32|psi64>|^2 without renormalising; the
+    same gate parameters, in double, for both).  The TF32 engines truncate in
+    their FP32 accumulation; their drift is bounded here as documented."""
+    n, depth = 18, 100
+    r128 = W.brick(n, depth, seed=5).gate_records(np.complex128)
+    x = np.zeros(1 << n, dtype=np.complex128)
+    x[0] = 1
+    ref = run_gpu(states, n, np.complex128, r128, "N", 0, x, fused=True)
+    for opts, bound in ((None, 1e-6), (L.FuseOpts(engine=4), 1e-3)):
+        y = run_gpu(states, n, np.complex64, r128, "N", 0, x.astype(np.complex64), fused=True,
+                    opts=opts).astype(np.complex128)
+        infid = 1.0 - abs(np.vdot(ref, y)) ** 2
+        assert abs(infid) < bound, (opts and opts.engine, infid)
+        assert abs(np.vdot(y, y).real - 1.0) < bound
 
 
 def test_qft20_config(states):

@@ -7,7 +7,7 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("dtype,engine", [("c128", 0), ("c128", 1), ("c64", 0), ("c64", 2),
-                                          ("c64", 3)])
+                                          ("c64", 3), ("c64", 4)])
 def test_sweep_command(cuda, dtype, engine):
     out = sweep.main(["--qubits", "14", "--depth", "6", "--dtype", dtype, "--engine",
                       str(engine), "--repeat", "1"])
