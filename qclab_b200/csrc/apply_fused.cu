@@ -18,6 +18,7 @@
 #include <array>
 #include <complex>
 #include <initializer_list>
+#include <thread>
 #include <type_traits>
 #include <cstring>
 #include <unordered_map>
@@ -962,26 +963,43 @@ int dmma_pass_bits(int m) { return (QSV_DMMA_BITS == 3 && m >= 8) ? 3 : 2; }
 // The tensor-core engine's plan.  A dense pass costs the same whatever it
 // holds, and the pass count depends strongly on which low bits every tile
 // keeps (brick circuits: 1982 passes with 2 low bits, 1782 with 3, for 30
-// qubits and 12 tile bits); so when the caller leaves low_bits unset, the
-// default and one more contiguous low bit are both planned and the plan
-// with fewer passes (then fewer stages) is kept.
+// qubits and 12 tile bits).  So when the caller leaves low_bits unset, the
+// default and more contiguous low bits are planned (in parallel host
+// threads) and the plan with the least passes + kappa * stages is kept: a
+// stage's tile load and store cost about one pass for 16-byte amplitudes
+// and a quarter of one for 8-byte amplitudes (fitted from 29-qubit brick
+// sweeps on a B200: complex<double> 862 passes/154 stages 1100 ms against
+// 837/193 1121 ms; complex<float> 853/150 962 ms against 826/182 940 ms).
 qsv_status pack_dense_plan(const std::vector<Lowered>& items, int n, int m, int low,
-                           bool low_fixed, int R, int max_gates, PackedPlan<double2>* plan,
-                           int* low_used) {
-  *low_used = low;
-  if (qsv_status st = pack_plan<double2>(items, n, m, low, R, max_gates, plan, 1, kDmmaPlanMax,
-                                         QSV_DENSE_SEARCH != 0))
-    return st;
-  if (low_fixed || low + 1 > m || QSV_DENSE_LOW_SEARCH == 0) return QSV_SUCCESS;
-  PackedPlan<double2> alt;
-  if (pack_plan<double2>(items, n, m, low + 1, R, max_gates, &alt, 1, kDmmaPlanMax,
-                         QSV_DENSE_SEARCH != 0) != QSV_SUCCESS)
-    return QSV_SUCCESS;  // keep the first plan
-  if (alt.passes.size() < plan->passes.size() ||
-      (alt.passes.size() == plan->passes.size() && alt.stages.size() < plan->stages.size())) {
-    *plan = std::move(alt);
-    *low_used = low + 1;
+                           bool low_fixed, int R, int max_gates, size_t elem_bytes,
+                           PackedPlan<double2>* plan, int* low_used) {
+  std::vector<int> lows = {low};
+  if (!low_fixed && QSV_DENSE_LOW_SEARCH) {
+    const int extra = elem_bytes >= 16 ? 1 : 3;
+    for (int d = 1; d <= extra && low + d < m; ++d) lows.push_back(low + d);
   }
+  std::vector<PackedPlan<double2>> plans(lows.size());
+  std::vector<qsv_status> status(lows.size(), QSV_SUCCESS);
+  std::vector<std::thread> workers;
+  for (size_t i = 1; i < lows.size(); ++i)
+    workers.emplace_back([&, i] {
+      status[i] = pack_plan<double2>(items, n, m, lows[i], R, max_gates, &plans[i], 1,
+                                     kDmmaPlanMax, QSV_DENSE_SEARCH != 0);
+    });
+  status[0] = pack_plan<double2>(items, n, m, lows[0], R, max_gates, &plans[0], 1, kDmmaPlanMax,
+                                 QSV_DENSE_SEARCH != 0);
+  for (std::thread& t : workers) t.join();
+  if (status[0] != QSV_SUCCESS) return status[0];
+  const double kappa = elem_bytes >= 16 ? 1.0 : 0.25;
+  size_t best = 0;
+  double best_cost = 0.0;
+  for (size_t i = 0; i < lows.size(); ++i) {
+    if (status[i] != QSV_SUCCESS) continue;
+    const double cost = (double)plans[i].passes.size() + kappa * (double)plans[i].stages.size();
+    if (i == 0 || cost < best_cost) { best = i; best_cost = cost; }
+  }
+  *plan = std::move(plans[best]);
+  *low_used = lows[best];
   return QSV_SUCCESS;
 }
 
@@ -996,7 +1014,8 @@ qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool v
   // plans sized per launch: a few KB typically, at most kDmmaPlanMax
   if ((size_t(1) << m) * sizeof(V) + kDmmaPlanMax > 200 * 1024) return QSV_ERROR_NOT_SUPPORTED;
   const bool low_fixed = x.opts && x.opts->low_bits > 0;
-  if (qsv_status st = pack_dense_plan(*x.items, n, m, low, low_fixed, R, max_gates, &plan, &low))
+  if (qsv_status st = pack_dense_plan(*x.items, n, m, low, low_fixed, R, max_gates, sizeof(V), &plan,
+                                      &low))
     return st;
   if (plan.stages.empty()) return QSV_SUCCESS;
   // complex<float> three-bit passes run on FP64 MMA like complex<double>
@@ -1291,7 +1310,7 @@ qsv_status plan_counts(const std::vector<Lowered>& low, int n, const qsv_fuse_op
     fx::PackedPlan<double2> plan;
     int low_used = lowb;
     if (qsv_status st = pack_dense_plan(low, n, md, lowb, opts && opts->low_bits > 0,
-                                            dmma_pass_bits(md), max_gates, &plan, &low_used))
+                                        dmma_pass_bits(md), max_gates, sizeof(V), &plan, &low_used))
       return st;
     for (const fx::PackedStage& ps : plan.stages) {
       ops->push_back(ps.nops);

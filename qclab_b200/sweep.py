@@ -45,6 +45,7 @@ def main(argv=None) -> dict:
     p.add_argument("--dtype", choices=sorted(DTYPES), default="c128")
     p.add_argument("--engine", type=int, default=0)
     p.add_argument("--tile-bits", type=int, default=0)
+    p.add_argument("--low-bits", type=int, default=0)
     p.add_argument("--repeat", type=int, default=2)
     p.add_argument("--workload", choices=["brick", "adjoint", "batch"], default="brick")
     p.add_argument("--circuits", type=int, default=512)
@@ -55,7 +56,7 @@ def main(argv=None) -> dict:
         return _batch(a)
     dt, code = DTYPES[a.dtype]
     recs = W.brick(a.qubits, a.depth, seed=a.seed).gate_records(dt)
-    opts = L.FuseOpts(engine=a.engine, tile_bits=a.tile_bits)
+    opts = L.FuseOpts(engine=a.engine, tile_bits=a.tile_bits, low_bits=a.low_bits)
     lib = L.load()
     arr, ptr, cnt = L.gate_array(recs)
     ns, npas, nops = C.c_int(), C.c_int(), C.c_int()
