@@ -186,7 +186,9 @@ qsv_status qsv_last_stage_times(float* ms, int capacity, int* count);
 /* Plan statistics for a gate list (no device work): number of stages and
  * of ops per stage -- gates for the sparse engine (opts->engine = 1), one
  * dense matrix per register pass for the tensor-core engine.  stage_gates
- * may be NULL.                                                             */
+ * may be NULL.  With opts->low_bits unset, the tensor-core engine plans
+ * several low-bit counts and reports the plan it would run (the one with
+ * the least passes + a per-element-size weight of stages).                */
 qsv_status qsv_plan_stats(int nbQubits, qsv_dtype dtype, const qsv_gate* gates,
                           size_t nGates, char op, int offset,
                           const qsv_fuse_opts* opts, int* nStages,
