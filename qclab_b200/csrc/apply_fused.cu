@@ -970,11 +970,17 @@ int dmma_pass_bits(int m) { return (QSV_DMMA_BITS == 3 && m >= 8) ? 3 : 2; }
 // and a quarter of one for 8-byte amplitudes (fitted from 29-qubit brick
 // sweeps on a B200: complex<double> 862 passes/154 stages 1100 ms against
 // 837/193 1121 ms; complex<float> 853/150 962 ms against 826/182 940 ms).
+// States of fewer than 20 qubits, or of a single tile, keep the default.
 qsv_status pack_dense_plan(const std::vector<Lowered>& items, int n, int m, int low,
                            bool low_fixed, int R, int max_gates, size_t elem_bytes,
                            PackedPlan<double2>* plan, int* low_used) {
+  // Both searches (the rollout choice of pass bits and the low-bit
+  // candidates) only where they can pay: below 2^20 amplitudes the host
+  // planning (and threads) would cost more than the passes they save, and
+  // with one tile every low-bit choice gives the same plan.
+  const bool search = QSV_DENSE_SEARCH != 0 && n >= 20;
   std::vector<int> lows = {low};
-  if (!low_fixed && QSV_DENSE_LOW_SEARCH) {
+  if (!low_fixed && QSV_DENSE_LOW_SEARCH && n > m && n >= 20) {
     const int extra = elem_bytes >= 16 ? 1 : 3;
     for (int d = 1; d <= extra && low + d < m; ++d) lows.push_back(low + d);
   }
@@ -984,10 +990,10 @@ qsv_status pack_dense_plan(const std::vector<Lowered>& items, int n, int m, int 
   for (size_t i = 1; i < lows.size(); ++i)
     workers.emplace_back([&, i] {
       status[i] = pack_plan<double2>(items, n, m, lows[i], R, max_gates, &plans[i], 1,
-                                     kDmmaPlanMax, QSV_DENSE_SEARCH != 0);
+                                     kDmmaPlanMax, search);
     });
   status[0] = pack_plan<double2>(items, n, m, lows[0], R, max_gates, &plans[0], 1, kDmmaPlanMax,
-                                 QSV_DENSE_SEARCH != 0);
+                                 search);
   for (std::thread& t : workers) t.join();
   if (status[0] != QSV_SUCCESS) return status[0];
   const double kappa = elem_bytes >= 16 ? 1.0 : 0.25;
