@@ -974,11 +974,12 @@ int dmma_pass_bits(int m) { return (QSV_DMMA_BITS == 3 && m >= 8) ? 3 : 2; }
 qsv_status pack_dense_plan(const std::vector<Lowered>& items, int n, int m, int low,
                            bool low_fixed, int R, int max_gates, size_t elem_bytes,
                            PackedPlan<double2>* plan, int* low_used) {
-  // Both searches (the rollout choice of pass bits and the low-bit
-  // candidates) only where they can pay: below 2^20 amplitudes the host
-  // planning (and threads) would cost more than the passes they save, and
-  // with one tile every low-bit choice gives the same plan.
-  const bool search = QSV_DENSE_SEARCH != 0 && n >= 20;
+  // The low-bit candidates only where they can pay: below 2^20 amplitudes
+  // the extra plans (and threads) cost more host time than the passes they
+  // save, and with one tile every low-bit choice gives the same plan.  (The
+  // rollout choice of pass bits pays at every size: an adjoint loop over
+  // 8..18-qubit circuits ran 14.5 s with it, 16.5 s without.)
+  const bool search = QSV_DENSE_SEARCH != 0;
   std::vector<int> lows = {low};
   if (!low_fixed && QSV_DENSE_LOW_SEARCH && n > m && n >= 20) {
     const int extra = elem_bytes >= 16 ? 1 : 3;
