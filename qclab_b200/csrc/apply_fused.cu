@@ -970,18 +970,19 @@ int dmma_pass_bits(int m) { return (QSV_DMMA_BITS == 3 && m >= 8) ? 3 : 2; }
 // and a quarter of one for 8-byte amplitudes (fitted from 29-qubit brick
 // sweeps on a B200: complex<double> 862 passes/154 stages 1100 ms against
 // 837/193 1121 ms; complex<float> 853/150 962 ms against 826/182 940 ms).
-// States of fewer than 20 qubits, or of a single tile, keep the default.
+// States of fewer than 27 qubits, or of a single tile, keep the default.
 qsv_status pack_dense_plan(const std::vector<Lowered>& items, int n, int m, int low,
                            bool low_fixed, int R, int max_gates, size_t elem_bytes,
                            PackedPlan<double2>* plan, int* low_used) {
-  // The low-bit candidates only where they can pay: below 2^20 amplitudes
-  // the extra plans (and threads) cost more host time than the passes they
-  // save, and with one tile every low-bit choice gives the same plan.  (The
-  // rollout choice of pass bits pays at every size: an adjoint loop over
-  // 8..18-qubit circuits ran 14.5 s with it, 16.5 s without.)
+  // The low-bit candidates only where they can pay: an extra plan costs a
+  // few ms of host time for a thousand gates, which ~10 % fewer passes win
+  // back only from about 2^27 amplitudes on (a 26-qubit pass takes ~0.14 ms);
+  // with one tile every low-bit choice gives the same plan.  (The rollout
+  // choice of pass bits pays at every size: an adjoint loop over 8..18-qubit
+  // circuits ran 14.5 s with it, 16.5 s without.)
   const bool search = QSV_DENSE_SEARCH != 0;
   std::vector<int> lows = {low};
-  if (!low_fixed && QSV_DENSE_LOW_SEARCH && n > m && n >= 20) {
+  if (!low_fixed && QSV_DENSE_LOW_SEARCH && n > m && n >= 27) {
     const int extra = elem_bytes >= 16 ? 1 : 3;
     for (int d = 1; d <= extra && low + d < m; ++d) lows.push_back(low + d);
   }
