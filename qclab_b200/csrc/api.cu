@@ -255,7 +255,7 @@ qsv_status qsv_download(qsv_state s, void* host, size_t bytes) {
                               "download cudaMemcpyAsync");
   if (st) return st;
   if ((st = cuda_status(cudaStreamSynchronize(s->stream), "download synchronize"))) return st;
-  return tc_check_status();
+  return tc_check_status(s->stream);
 }
 
 qsv_status qsv_copy(qsv_state dst, qsv_state src) {
@@ -278,7 +278,7 @@ qsv_status qsv_set_basis(qsv_state s, uint64_t index) {
 qsv_status qsv_synchronize(qsv_state s) {
   if (qsv_status st = check_state(s)) return st;
   if (qsv_status st = cuda_status(cudaStreamSynchronize(s->stream), "qsv_synchronize")) return st;
-  return tc_check_status();
+  return tc_check_status(s->stream);
 }
 
 qsv_status qsv_apply(qsv_state s, const qsv_gate* gates, size_t nGates, char op, int offset) {

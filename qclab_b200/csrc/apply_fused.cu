@@ -1262,15 +1262,19 @@ int effective_tile_bits(size_t eb, int nv, int n, const qsv_fuse_opts* opts) {
 }
 int default_low_bits(size_t eb) { return eb >= 16 ? 2 : 3; }
 
-qsv_status tc_check_status() {
+qsv_status tc_check_status(cudaStream_t stream) {
   if (!g_tc_used.load(std::memory_order_relaxed)) return QSV_SUCCESS;
   unsigned v = 0;
-  if (qsv_status st = cuda_status(cudaMemcpyFromSymbol(&v, g_tc_status, sizeof(v)),
+  if (qsv_status st = cuda_status(cudaMemcpyFromSymbolAsync(&v, g_tc_status, sizeof(v), 0,
+                                                            cudaMemcpyDeviceToHost, stream),
                                   "tensor-core status read"))
     return st;
+  if (qsv_status st = cuda_status(cudaStreamSynchronize(stream), "tensor-core status read"))
+    return st;
   if (!v) return QSV_SUCCESS;
-  const unsigned zero = 0;
-  cudaMemcpyToSymbol(g_tc_status, &zero, sizeof(zero));
+  static const unsigned zero = 0;
+  cudaMemcpyToSymbolAsync(g_tc_status, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, stream);
+  cudaStreamSynchronize(stream);
   return fail(QSV_ERROR_TIMEOUT, "a tensor-core sweep gave up waiting for its MMAs (results invalid)");
 }
 

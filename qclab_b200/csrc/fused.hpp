@@ -29,8 +29,9 @@ int default_low_bits(size_t elem_bytes);
 qsv_status execute_fused(const ExecArgs& x);
 
 // QSV_ERROR_TIMEOUT once (and clears it) if a tcgen05 sweep's bounded wait
-// gave up since the last call; call after the stream has synchronised.
-qsv_status tc_check_status();
+// gave up since the last call; reads the device flag on `stream` (call after
+// that stream has synchronised; nothing is read before a tcgen05 launch).
+qsv_status tc_check_status(cudaStream_t stream);
 
 // Tile bits the executor uses for nv vectors of an n-qubit state: the
 // requested (or default) size, at most 14 and n, and at most 256 threads of
