@@ -4,8 +4,8 @@ reference's own outputs (golden fixtures), the CPU oracle, and each other.
 Tolerances:
 * reference-exact path (qsv_apply): bitwise equal (np.array_equal);
 * fused path (qsv_apply_fused): max-abs 1e-12 for complex128/float64 and
-  2e-5 for complex64/float32 on normalised states (the north-star bound is
-  1e-12 / 1e-5 at 30 qubits).
+  2e-5 for complex64/float32 on normalised states (the required bound for
+  the 30-qubit brick is 1e-12 / 1e-5).
 """
 import numpy as np
 import pytest
