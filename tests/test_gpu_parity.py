@@ -157,6 +157,25 @@ def test_complex_float_fused_keeps_the_norm(states):
         assert abs(np.vdot(y, y).real - 1.0) < bound
 
 
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=lambda d: np.dtype(d).name)
+def test_fused_small_states_and_empty_lists(states, dtype):
+    """1..9 qubits cross every engine boundary (sparse passes below 7 tile
+    bits, 2-bit FP64 MMA at 7, 3-bit passes above, the TF32 engines for
+    complex<float>); an empty gate list leaves the state untouched."""
+    for n in range(1, 10):
+        rng = np.random.default_rng(100 + n)
+        recs = W.random_mixed(n, 40, seed=n).gate_records(dtype)
+        x = (rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)).astype(dtype)
+        x /= np.linalg.norm(x)
+        ref = oracle.apply(x.copy(), recs, "N")
+        for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=3), L.FuseOpts(engine=4)):
+            y = run_gpu(states, n, dtype, recs, "N", 0, x, fused=True, opts=opts)
+            assert np.max(np.abs(y - ref)) <= tol(dtype), (n, opts and opts.engine)
+        for fused in (False, True):
+            y = run_gpu(states, n, dtype, recs[:0], "N", 0, x, fused=fused)
+            assert np.array_equal(y, x), (n, fused)
+
+
 def test_qft20_config(states):
     """Plain QFT on 20 qubits, complex<double>, basis input from a seed."""
     n = 20
