@@ -269,8 +269,16 @@ qsv_status pack_plan(const std::vector<Lowered>& gates, int n, int m, int low, i
         for (const POp& q : B.ops) host_apply_pop(x, B.r, q, B.c64.data() + q.coef);
         for (int i = 0; i < N; ++i) U[size_t(k) * N + i] = x[i];
       }
+      bool real = true, diagonal = true;
+      for (int k = 0; k < N; ++k)
+        for (int i = 0; i < N; ++i) {
+          const cplxd z = U[size_t(k) * N + i];
+          if (z.imag() != 0.0) real = false;
+          if (i != k && z != cplxd(0.0, 0.0)) diagonal = false;
+        }
       POp d{};
       d.shape = P_DENSE;
+      d.form = diagonal ? kDenseDiagonal : (real ? kDenseReal : kDenseGeneral);
       d.coef = 0;
       B.ops.assign(1, d);
       B.coefs.clear();
@@ -506,6 +514,30 @@ __global__ void __launch_bounds__(256, 2) k_dmma3(V* __restrict__ v0, DmmaArgs a
     const PassDev& P = passes[pi];
     const uint16_t* T = P.off;
     const double2* U = coefs + ops[P.op0].coef;        // U[i][k] at k * 8 + i
+    const int form = ops[P.op0].form;                   // uniform over the block
+    if (form == kDenseDiagonal) {
+      // out_j = U[j][j] x_j, in place: lane (q, k4) owns amplitudes k4 and
+      // 4 + k4 of group q in every column tile
+      const double2 d0 = U[k4 * 8 + k4], d1 = U[(4 + k4) * 8 + 4 + k4];
+      const uint32_t in0 = (uint32_t)T[4 + q] ^ T[12 + k4];
+      const uint32_t in1 = (uint32_t)T[4 + q] ^ T[12 + 4 + k4];
+      for (uint32_t c = warp; c < nchunks; c += nwarps) {
+        uint32_t cb = 0;
+        for (uint32_t cc = c, k = 0; cc; cc >>= 1, ++k)
+          if (cc & 1u) cb ^= T[20 + k];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const uint32_t tb = cb ^ T[t];
+          const double2 x0 = to_d2(t0[tb ^ in0]), x1 = to_d2(t0[tb ^ in1]);
+          t0[tb ^ in0] = from_d2<V>(make_double2(fma(d0.x, x0.x, -d0.y * x0.y),
+                                                 fma(d0.x, x0.y, d0.y * x0.x)));
+          t0[tb ^ in1] = from_d2<V>(make_double2(fma(d1.x, x1.x, -d1.y * x1.y),
+                                                 fma(d1.x, x1.y, d1.y * x1.x)));
+        }
+      }
+      __syncthreads();
+      continue;
+    }
     const double2 ulo = U[k4 * 8 + q], uhi = U[(4 + k4) * 8 + q];
     double A[2][4];
 #pragma unroll

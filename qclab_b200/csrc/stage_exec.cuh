@@ -85,6 +85,9 @@ enum Form : int8_t {
 };
 
 enum POpShape : int8_t { P_PAIR = 1, P_CPAIR = 2, P_MUL = 3, P_QUAD = 4, P_RED = 5, P_DENSE = 6 };
+// POp.form of a P_DENSE op: the structure of its matrix U (exact zeros of
+// the FP64 product), which the tensor-core kernel uses to skip MMAs
+constexpr int8_t kDenseGeneral = 0, kDenseReal = 1, kDenseDiagonal = 2;
 
 // One op of a register pass; positions index the pass's register bits.
 struct POp {
