@@ -317,55 +317,82 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_reference_sample(n, recs, budget_s=15.0):
-    """QCLAB++'s CPU simulate (oracle/_ref, all host threads) on a bounded
-    slice of the circuit; returns (gates/s, threads, kind, sample text)."""
-    import oracle
-    dtype = np.complex128
-    kind = "reference" if oracle.ref_available() else "port"
-    if kind == "port":
-        # the C oracle: single-threaded restatement; time a slice at 24 qubits
-        n_s = min(n, 24)
-        from qclab_b200 import workloads as W
-        sub = [r for r in recs if max(r["qubit0"], r["qubit1"]) < n_s][:200]
-        sub = np.array(sub, dtype=recs.dtype)
-        x = np.zeros(1 << n_s, dtype=dtype)
-        x[0] = 1
+class CpuBrickSample:
+    """QCLAB++'s CPU simulate (oracle/_ref, OpenMP, all host threads) timed
+    on WHOLE brick layers of the circuit, so the sample has the circuit's own
+    gate mix (per layer n one-qubit gates, which stream the state twice, and
+    n/2 CNOT/CZ, which stream it once or half).  The state is allocated and
+    first-touched once, outside the timed calls; each ``run()`` resets it to
+    |0...0> (untimed) and times QCircuit::simulate over the sampled layers.
+    Without oracle/_ref the C restatement (one thread) is timed instead at
+    24 qubits on whole layers of a 24-qubit brick and scaled by 2^(n-24)."""
+
+    def __init__(self, n, recs, layer_sizes, budget_s=15.0):
+        import oracle
+        self.oracle = oracle
+        self.n = n
+        self.kind = "reference" if oracle.ref_available() else "port"
+        if self.kind == "port":
+            from qclab_b200 import workloads as W
+            self.n_s = min(n, 24)
+            sizes = W.brick_layer_sizes(self.n_s, 2)
+            self.recs = W.brick(self.n_s, 2, seed=0).gate_records(np.complex128)
+            self.layers = 2
+            self.threads = 1
+            self.x = np.zeros(1 << self.n_s, dtype=np.complex128)
+            self.gates = sum(sizes)
+            return
+        try:
+            import psutil
+            avail = psutil.virtual_memory().available
+        except Exception:
+            avail = 1 << 40
+        self.n_s = n
+        while self.n_s > 20 and (1 << self.n_s) * 16 * 2.5 > avail:
+            self.n_s -= 1
+        # size the sample from one timed layer: as many whole layers as fit the budget
+        first = recs[:layer_sizes[0]]
+        rc = oracle.RefCircuit(self.n_s, np.complex128, first)
+        rc.state[:] = 0
+        rc.state[0] = 1
         t0 = time.perf_counter()
-        oracle.apply(x, sub)
-        dt = time.perf_counter() - t0
-        return len(sub) / dt * (1 << n_s) / (1 << n), 1, kind, (
-            f"C oracle, 1 thread, first {len(sub)} gates at {n_s} qubits, scaled by 2^{n - n_s}")
-    try:
-        import psutil
-        avail = psutil.virtual_memory().available
-    except Exception:
-        avail = 1 << 40
-    n_s = n
-    while n_s > 20 and (1 << n_s) * 16 * 2.5 > avail:
-        n_s -= 1
-    # one gate first to size the sample
-    one = oracle.RefCircuit(n_s, dtype, recs[:1])
-    one.state[:] = 0
-    one.state[0] = 1
-    t0 = time.perf_counter()
-    one.apply()
-    per_gate = time.perf_counter() - t0
-    one.close()
-    g = int(max(5, min(len(recs), budget_s / max(per_gate, 1e-6))))
-    sub = recs[:g]
-    rc = oracle.RefCircuit(n_s, dtype, sub)
-    rc.state[:] = 0
-    rc.state[0] = 1
-    t0 = time.perf_counter()
-    rc.apply()
-    dt = time.perf_counter() - t0
-    threads = oracle.ref_threads()
-    rc.close()
-    scale = (1 << n_s) / (1 << n)
-    txt = (f"QCLAB++ QCircuit::simulate (g++ -O3 -fopenmp), {threads} threads, first {g} gates "
-           f"of the circuit at {n_s} qubits" + (f", scaled by 2^{n - n_s}" if n_s != n else ""))
-    return g / dt * scale, threads, kind, txt
+        rc.apply()
+        per_layer = time.perf_counter() - t0
+        rc.close()
+        self.layers = int(max(1, min(len(layer_sizes), budget_s // max(per_layer, 1e-6))))
+        self.gates = sum(layer_sizes[:self.layers])
+        self.rc = oracle.RefCircuit(self.n_s, np.complex128, recs[:self.gates])
+        self.threads = oracle.ref_threads()
+
+    def run(self):
+        """Gates/s of one timed simulate over the sampled layers."""
+        if self.kind == "port":
+            self.x[:] = 0
+            self.x[0] = 1
+            t0 = time.perf_counter()
+            self.oracle.apply(self.x, self.recs)
+            dt = time.perf_counter() - t0
+        else:
+            self.rc.state[:] = 0
+            self.rc.state[0] = 1
+            t0 = time.perf_counter()
+            self.rc.apply()
+            dt = time.perf_counter() - t0
+        return self.gates / dt * (1 << self.n_s) / (1 << self.n)
+
+    def describe(self):
+        if self.kind == "port":
+            return (f"C oracle, 1 thread, 2 whole brick layers ({self.gates} gates) at "
+                    f"{self.n_s} qubits, scaled by 2^{self.n - self.n_s}")
+        return (f"QCLAB++ QCircuit::simulate (g++ -O3 -fopenmp), {self.threads} threads, the "
+                f"first {self.layers} whole brick layer(s) ({self.gates} gates, the circuit's "
+                f"gate mix) at {self.n_s} qubits"
+                + (f", scaled by 2^{self.n - self.n_s}" if self.n_s != self.n else ""))
+
+    def close(self):
+        if getattr(self, "rc", None) is not None:
+            self.rc.close()
+            self.rc = None
 
 
 def run_reference_arm(args, rank, world):
@@ -373,13 +400,16 @@ def run_reference_arm(args, rank, world):
         return
     from qclab_b200 import workloads as W
     recs = W.brick(args.qubits, args.depth, seed=args.seed).gate_records(np.complex128)
+    sample = CpuBrickSample(args.qubits, recs, W.brick_layer_sizes(args.qubits, args.depth),
+                            budget_s=8.0)
     vals = []
-    threads, kind, txt = 0, "reference", ""
     for i in range(args.warmup + args.steps):
-        v, threads, kind, txt = cpu_reference_sample(args.qubits, recs, budget_s=8.0)
+        v = sample.run()
         if i >= args.warmup:
             vals.append(v)
+    sample.close()
     value = statistics.median(vals)
+    threads, kind, txt = sample.threads, sample.kind, sample.describe()
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "gates/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -578,8 +608,11 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, threads, kind, txt = cpu_reference_sample(n, recs)
-        cpu = {"value": v, "unit": "gates/s", "cores": threads, "kind": kind, "sample": txt}
+        sample = CpuBrickSample(n, recs, W.brick_layer_sizes(n, args.depth))
+        v = sample.run()
+        cpu = {"value": v, "unit": "gates/s", "cores": sample.threads, "kind": sample.kind,
+               "sample": sample.describe()}
+        sample.close()
 
     sv.close()
     extras = {}

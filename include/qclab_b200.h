@@ -6,7 +6,10 @@
  * qsv_last_error() returns a message for the last failure on the calling
  * thread.  All device work is issued on the state's CUDA stream (the legacy
  * default stream unless qsv_set_stream was called); calls that return host
- * values (downloads, reductions) synchronise that stream.
+ * values (downloads, reductions) synchronise that stream.  Calls on two
+ * states with different streams order themselves on the device: the work
+ * starts after both streams' earlier work, and later work on either stream
+ * starts after it (CUDA events, no host synchronisation).
  *
  * Conventions follow QCLAB++ exactly:
  *   - qubit q of an n-qubit register is bit (n-1-q) of the amplitude index
@@ -130,6 +133,7 @@ qsv_status qsv_info(qsv_state state, int* nbQubits, qsv_dtype* dtype,
                     void** device_ptr);
 qsv_status qsv_upload(qsv_state state, const void* host, size_t bytes);
 qsv_status qsv_download(qsv_state state, void* host, size_t bytes);
+/* dst <- src (same size and dtype), issued on dst's stream. */
 qsv_status qsv_copy(qsv_state dst, qsv_state src);
 /* |index> (a computational basis state, big-endian qubit order). */
 qsv_status qsv_set_basis(qsv_state state, uint64_t index);
@@ -231,7 +235,8 @@ qsv_status qsv_expectation(qsv_state state, const char* paulis,
  * this library would fail or fragment that pool), or a tight optimisation
  * loop that cannot afford cudaMalloc/cudaFree, which synchronise the
  * device.  No counterpart in the reference (QCLAB++ has no observables).
- *   state       : caller-owned device array of 2^nbQubits elements of dtype.
+ *   state       : caller-owned device array of 2^nbQubits elements of dtype,
+ *                 on the current device (QSV_ERROR_INVALID_VALUE otherwise).
  *   cuda_stream : stream to run on (NULL = legacy default stream); the call
  *                 synchronises it before returning.
  * Calls no cudaMalloc/cudaFree: its work memory is a fixed 1 MiB array
@@ -246,7 +251,8 @@ qsv_status qsv_expectation_noalloc(const void* state, int nbQubits,
                                    qsv_dtype dtype, void* cuda_stream,
                                    const char* paulis, const double* coefs,
                                    size_t nTerms, double* out);
-/* dst = H src (dst != src, same size and dtype; products formed in FP64). */
+/* dst = H src (dst != src, same size and dtype; products formed in FP64),
+ * issued on src's stream. */
 qsv_status qsv_apply_observable(qsv_state dst, qsv_state src,
                                 const char* paulis, const double* coefs,
                                 size_t nTerms);

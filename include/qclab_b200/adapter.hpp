@@ -244,17 +244,32 @@ void simulate(const qclab::QCircuit<T, G>& c, std::vector<T>& vector, bool fused
   apply<T>(c, qclab::Op::NoTrans, c.nbQubits(), vector, 0, fused);
 }
 
-// circuit.simulate_device(ptr): in place on caller-owned device memory.
-template <typename T, typename G>
-void simulate_device(const qclab::QCircuit<T, G>& c, T* device_vector, bool fused = false) {
-  const std::vector<qsv_gate> g = records<T>(c, 0);
+// obj.apply_device(op, nbQubits, device_vector, offset) -- the QObject<T>
+// virtual of the offload build (include/qclab/QObject.hpp:56-59) and its
+// QCircuit<T,G> loop (include/qclab/QCircuit.hpp:146-160): in place on
+// caller-owned device memory of 2^nbQubits elements of T on the current
+// device; the gate list runs in reverse order for [Conj]Trans and every gate
+// gets the circuits' offset_ plus `offset`.  Returns after the device work
+// has finished, as the reference's synchronous offload loops do.
+template <typename T>
+void apply_device(const qclab::QObject<T>& o, qclab::Op op, int nbQubits, T* device_vector,
+                  int offset = 0, bool fused = false) {
+  const std::vector<qsv_gate> g = records<T>(o, 0);
   qsv_state s = nullptr;
-  check(qsv_wrap(c.nbQubits(), dtype_of<T>(), device_vector, &s), "qsv_wrap");
-  qsv_status st = fused ? qsv_apply_fused(s, g.data(), g.size(), 'N', 0, nullptr)
-                        : qsv_apply(s, g.data(), g.size(), 'N', 0);
+  check(qsv_wrap(nbQubits, dtype_of<T>(), device_vector, &s), "qsv_wrap");
+  const char opc = static_cast<char>(op);
+  qsv_status st = fused ? qsv_apply_fused(s, g.data(), g.size(), opc, offset, nullptr)
+                        : qsv_apply(s, g.data(), g.size(), opc, offset);
   if (st == QSV_SUCCESS) st = qsv_synchronize(s);
   qsv_destroy(s);
-  check(st, "qclab_b200::simulate_device");
+  check(st, "qclab_b200::apply_device");
+}
+
+// circuit.simulate_device(ptr) (include/qclab/QCircuit.hpp:169-172): in place
+// on caller-owned device memory.
+template <typename T, typename G>
+void simulate_device(const qclab::QCircuit<T, G>& c, T* device_vector, bool fused = false) {
+  apply_device<T>(c, qclab::Op::NoTrans, c.nbQubits(), device_vector, 0, fused);
 }
 
 }  // namespace qclab_b200

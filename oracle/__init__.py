@@ -33,11 +33,28 @@ _lib = None
 _ref = None
 
 
+def ref_tree() -> Path | None:
+    """The QCLAB++ source tree: $QCLAB_REF, else the tree the last build of
+    _ref/ used (recorded in _ref/REF_TREE); None when neither exists."""
+    cands = [os.environ.get("QCLAB_REF", "")]
+    rec = HERE / "_ref" / "REF_TREE"
+    if rec.exists():
+        cands.append(rec.read_text().strip())
+    for c in cands:
+        if c and (Path(c) / "src" / "qgates" / "apply.hpp").exists():
+            return Path(c)
+    return None
+
+
 def build() -> None:
-    """Builds liboracle.so (always) and _ref/ (when the reference tree exists)."""
+    """Builds liboracle.so (always) and _ref/ (when ref_tree() finds the
+    reference tree)."""
     env = dict(os.environ)
     env.pop("CC", None)
     env.pop("CXX", None)
+    tree = ref_tree()
+    if tree is not None:
+        env["QCLAB_REF"] = str(tree)
     r = subprocess.run(["make", "-C", str(HERE), "-j8", "all"], capture_output=True, text=True,
                        env=env)
     if r.returncode != 0:

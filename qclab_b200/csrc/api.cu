@@ -35,6 +35,18 @@ qsv_status cuda_status(cudaError_t e, const char* what) {
 
 void count_launch(uint64_t k) { g_launches += k; }
 
+qsv_status stream_wait(cudaStream_t waiter, cudaStream_t producer) {
+  if (waiter == producer) return QSV_SUCCESS;
+  cudaEvent_t ev;
+  if (qsv_status st = cuda_status(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming),
+                                  "cudaEventCreateWithFlags"))
+    return st;
+  qsv_status st = cuda_status(cudaEventRecord(ev, producer), "cudaEventRecord");
+  if (!st) st = cuda_status(cudaStreamWaitEvent(waiter, ev, 0), "cudaStreamWaitEvent");
+  cudaEventDestroy(ev);  // released once the recorded work completes
+  return st;
+}
+
 qsv_status ensure_aux(qsv_state_s* s, size_t bytes) {
   if (s->aux_bytes >= bytes) return QSV_SUCCESS;
   if (s->aux) {
@@ -264,8 +276,13 @@ qsv_status qsv_copy(qsv_state dst, qsv_state src) {
   if (dst->n != src->n || dst->dtype != src->dtype)
     return fail(QSV_ERROR_SIZE, "qsv_copy: states differ in size or dtype");
   const size_t bytes = dim(src->n) * elem_bytes(src->dtype);
-  return cuda_status(cudaMemcpyAsync(dst->d, src->d, bytes, cudaMemcpyDeviceToDevice, dst->stream),
-                     "qsv_copy");
+  // the copy runs on dst's stream: after src's pending work, and src's
+  // later work waits for the copy to finish reading it
+  if (qsv_status st = stream_wait(dst->stream, src->stream)) return st;
+  if (qsv_status st = cuda_status(cudaMemcpyAsync(dst->d, src->d, bytes, cudaMemcpyDeviceToDevice,
+                                                  dst->stream), "qsv_copy"))
+    return st;
+  return stream_wait(src->stream, dst->stream);
 }
 
 qsv_status qsv_set_basis(qsv_state s, uint64_t index) {

@@ -644,10 +644,11 @@ qsv_status qsv_apply_observable(qsv_state dst, qsv_state src, const char* paulis
     return fail(QSV_ERROR_INVALID_VALUE, "qsv_apply_observable needs distinct states");
   if (dst->n != src->n || dst->dtype != src->dtype)
     return fail(QSV_ERROR_SIZE, "states differ in size or dtype");
-  if (dst->stream != src->stream)
-    if (qsv_status st = cuda_status(cudaStreamSynchronize(dst->stream), "observable stream sync"))
-      return st;
-  return observable_internal(dst, src, paulis, coefs, nterms);
+  // dst is written on src's stream: after dst's pending work, and dst's
+  // later work waits for the write
+  if (qsv_status st = stream_wait(src->stream, dst->stream)) return st;
+  if (qsv_status st = observable_internal(dst, src, paulis, coefs, nterms)) return st;
+  return stream_wait(dst->stream, src->stream);
 }
 
 }  // extern "C"
@@ -859,6 +860,19 @@ extern "C" qsv_status qsv_expectation_noalloc(const void* state, int nbQubits, q
     return fail(QSV_ERROR_SIZE, "nbQubits %d outside [1,%d]", nbQubits, kMaxQubits);
   std::vector<HTerm> T;
   if (qsv_status st = parse_terms(nbQubits, paulis, coefs, nTerms, &T)) return st;
+  // the state must live on the current device, whose copy of the work array
+  // the kernels use
+  cudaPointerAttributes attr{};
+  if (qsv_status st = cuda_status(cudaPointerGetAttributes(&attr, state),
+                                  "cudaPointerGetAttributes(state)"))
+    return st;
+  int dev = 0;
+  if (qsv_status st = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return st;
+  if (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged)
+    return fail(QSV_ERROR_INVALID_VALUE, "qsv_expectation_noalloc: state is not device memory");
+  if (attr.type == cudaMemoryTypeDevice && attr.device != dev)
+    return fail(QSV_ERROR_INVALID_VALUE,
+                "qsv_expectation_noalloc: state on device %d, current device %d", attr.device, dev);
   cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
   switch (dtype) {
     case QSV_C128: return expect_noalloc_typed<double2>((const double2*)state, nbQubits, stream, T, out);

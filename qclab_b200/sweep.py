@@ -37,7 +37,9 @@ from .state import StateVector
 DTYPES = {"c128": (np.complex128, L.C128), "c64": (np.complex64, L.C64)}
 
 
-def main(argv=None) -> dict:
+def main(argv=None, keep_state: bool = False) -> dict:
+    """Runs the command; with ``keep_state`` the returned dict also holds
+    the last sweep's final state (``state``, a host array; not printed)."""
     p = argparse.ArgumentParser(prog="python -m qclab_b200.sweep")
     p.add_argument("--qubits", type=int, default=26)
     p.add_argument("--depth", type=int, default=40)
@@ -75,9 +77,12 @@ def main(argv=None) -> dict:
             s.apply(recs, "N", 0, fused=True, opts=opts)
             s.synchronize()
             ms.append((time.perf_counter() - t) * 1e3)
+        final = s.download() if keep_state else None
     out["ms"] = [round(v, 3) for v in ms]
     out["gates_per_s"] = cnt / (min(ms) / 1e3) if ms else None
     print(json.dumps(out), flush=True)
+    if keep_state:
+        out["state"] = final
     return out
 
 

@@ -60,6 +60,12 @@ def brick(n: int, depth: int, seed: int = 0) -> QCircuit:
     return c
 
 
+def brick_layer_sizes(n: int, depth: int) -> list[int]:
+    """Gates per layer of ``brick(n, depth)``: n one-qubit gates plus one
+    two-qubit gate per pair (q, q+1), q of the layer's parity."""
+    return [n + len(range(layer % 2, n - 1, 2)) for layer in range(depth)]
+
+
 def hea(n: int, layers: int, seed: int = 0) -> QCircuit:
     rng = np.random.default_rng(seed)
     c = QCircuit(n)

@@ -6,6 +6,8 @@
 #include <cstdio>
 #include <random>
 
+#include <cuda_runtime.h>
+
 #include "qclab_b200/adapter.hpp"
 
 using namespace qclab::qgates;
@@ -59,6 +61,77 @@ int run(const char* name, const qclab::QCircuit<T>& c, std::mt19937_64& rng, boo
     std::printf("%-28s op=%c fused=%d max_abs=%.3e %s\n", name, opc, (int)fused, err,
                 ok ? "ok" : "FAIL");
   }
+  return bad;
+}
+
+// apply_device / simulate_device on cudaMalloc'd memory (the offload
+// build's device-pointer surface) against QCLAB++'s CPU apply/simulate, for
+// every op and a nonzero offset (the object acting on the upper qubits of a
+// larger register).
+template <typename T>
+int run_device(const char* name, const qclab::QCircuit<T>& c, std::mt19937_64& rng, bool fused) {
+  const int n = c.nbQubits() + 2, off = 2;
+  std::normal_distribution<double> N01;
+  std::vector<T> v(size_t(1) << n);
+  for (auto& x : v) {
+    if constexpr (qclab::is_complex_v<T>) x = T(N01(rng), N01(rng));
+    else x = T(N01(rng));
+  }
+  const size_t bytes = v.size() * sizeof(T);
+  T* d = nullptr;
+  if (cudaMalloc(&d, bytes) != cudaSuccess) {
+    std::printf("%-28s cudaMalloc failed\n", name);
+    return 1;
+  }
+  const double tol = sizeof(qclab::real_t<T>) == 8 ? 1e-10 : 5e-5;
+  int bad = 0;
+  auto compare = [&](const char* what, char opc, const std::vector<T>& ref) {
+    std::vector<T> gpu(v.size());
+    cudaMemcpy(gpu.data(), d, bytes, cudaMemcpyDeviceToHost);
+    double err = 0;
+    bool same = true;
+    for (size_t i = 0; i < v.size(); ++i) {
+      err = std::max(err, (double)std::abs(ref[i] - gpu[i]));
+      same = same && (ref[i] == gpu[i]);
+    }
+    const bool ok = fused ? err <= tol : same;
+    if (!ok) ++bad;
+    std::printf("%-28s %-15s op=%c fused=%d max_abs=%.3e %s\n", name, what, opc, (int)fused, err,
+                ok ? "ok" : "FAIL");
+  };
+  for (char opc : {'N', 'T', 'C'}) {
+    const qclab::Op op = static_cast<qclab::Op>(opc);
+    std::vector<T> ref = v;
+    c.apply(op, n, ref, off);  // QCLAB++ CPU path
+    cudaMemcpy(d, v.data(), bytes, cudaMemcpyHostToDevice);
+    qclab_b200::apply_device(c, op, n, d, off, fused);
+    compare("apply_device", opc, ref);
+  }
+  {
+    std::vector<T> w(size_t(1) << c.nbQubits());
+    for (auto& x : w) {
+      if constexpr (qclab::is_complex_v<T>) x = T(N01(rng), N01(rng));
+      else x = T(N01(rng));
+    }
+    std::vector<T> ref = w;
+    c.simulate(ref);
+    v = w;
+    cudaMemcpy(d, w.data(), w.size() * sizeof(T), cudaMemcpyHostToDevice);
+    qclab_b200::simulate_device(c, d, fused);
+    std::vector<T> gpu(w.size());
+    cudaMemcpy(gpu.data(), d, w.size() * sizeof(T), cudaMemcpyDeviceToHost);
+    double err = 0;
+    bool same = true;
+    for (size_t i = 0; i < w.size(); ++i) {
+      err = std::max(err, (double)std::abs(ref[i] - gpu[i]));
+      same = same && (ref[i] == gpu[i]);
+    }
+    const bool ok = fused ? err <= tol : same;
+    if (!ok) ++bad;
+    std::printf("%-28s %-15s op=N fused=%d max_abs=%.3e %s\n", name, "simulate_device",
+                (int)fused, err, ok ? "ok" : "FAIL");
+  }
+  cudaFree(d);
   return bad;
 }
 
@@ -126,6 +199,8 @@ int main() {
     }
     bad += run("mixed12-complex<double>", mixed<C>(12, 1), rng, fused);
     bad += run("mixed10-complex<float>", mixed<F>(10, 2), rng, fused);
+    bad += run_device("device-mixed11-c<double>", mixed<C>(11, 3), rng, fused);
+    bad += run_device("device-mixed9-c<float>", mixed<F>(9, 4), rng, fused);
   }
   std::printf("adapter_test: %s\n", bad ? "FAILED" : "all passed");
   return bad ? 1 : 0;

@@ -4,11 +4,13 @@ from pathlib import Path
 
 import pytest
 
+import oracle
+
 ROOT = Path(__file__).resolve().parent.parent
-REF = Path("/root/reference/include")
+TREE = oracle.ref_tree()
 
 
-@pytest.mark.skipif(not REF.exists(), reason="reference headers not present")
+@pytest.mark.skipif(TREE is None, reason="reference tree not present (set QCLAB_REF)")
 def test_adapter_header_compiles(tmp_path):
     src = tmp_path / "t.cpp"
     src.write_text('#include "qclab_b200/adapter.hpp"\n'
@@ -17,5 +19,5 @@ def test_adapter_header_compiles(tmp_path):
                    "template void qclab_b200::simulate(const qclab::QCircuit<float>&,"
                    " std::vector<float>&, bool);\n")
     r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", f"-I{ROOT / 'include'}",
-                        f"-I{REF}", str(src)], capture_output=True, text=True)
+                        f"-I{TREE / 'include'}", str(src)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-3000:]

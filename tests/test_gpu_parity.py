@@ -252,18 +252,31 @@ def test_circuit_offset_and_nesting(cuda):
 
 
 def test_wrap_caller_owned_device_memory(cuda):
-    """simulate_device(T*): the library works in place on caller memory."""
+    """simulate_device(T*): the library works in place on caller memory (a
+    torch allocation), bitwise like the oracle on a circuit over every gate
+    class, for every op, and within 1e-12 through the fused path."""
     import torch
-    from qclab_b200 import QCircuit, Hadamard
-    t = torch.zeros(16, dtype=torch.complex128, device="cuda")
-    t[0] = 1
-    sv = StateVector.wrap(t.data_ptr(), 4, np.complex128)
-    c = QCircuit(4)
-    for q in range(4):
-        c.push_back(Hadamard(q))
-    c.simulate_device(sv)
+    from qclab_b200 import QCircuit
+    n = 11
+    circ = W.random_mixed(n, 120, seed=17)
+    rng = np.random.default_rng(4)
+    x = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    x /= np.linalg.norm(x)
+    for op in ("N", "T", "C"):
+        t = torch.from_numpy(x.copy()).to("cuda")
+        sv = StateVector.wrap(t.data_ptr(), n, np.complex128)
+        circ.apply(op, n, sv)
+        sv.synchronize()
+        want = oracle.apply(x.copy(), circ.gate_records(np.complex128), op)
+        assert np.array_equal(t.cpu().numpy(), want), op
+        sv.close()
+    t = torch.from_numpy(x.copy()).to("cuda")
+    sv = StateVector.wrap(t.data_ptr(), n, np.complex128)
+    assert isinstance(circ, QCircuit)
+    circ.simulate_device(sv, fused=True)
     sv.synchronize()
-    assert torch.allclose(t.cpu(), torch.full((16,), 0.25, dtype=torch.complex128))
+    want = oracle.apply(x.copy(), circ.gate_records(np.complex128))
+    assert np.max(np.abs(t.cpu().numpy() - want)) < 1e-12
     sv.close()
 
 

@@ -109,3 +109,34 @@ def test_reduction_errors(cuda):
         with pytest.raises(QsvError) as e:
             a.expectation(H2)
         assert e.value.status == 1
+
+
+def test_copy_and_observable_across_streams(cuda):
+    """qsv_copy and qsv_apply_observable between two states whose streams
+    differ (non-blocking torch streams) order themselves on the device: each
+    is issued while a long circuit is still queued on the other state's
+    stream, and the source is overwritten right after the copy."""
+    import torch
+
+    from qclab_b200 import workloads as W
+    n = 20
+    recs = W.brick(n, 60, seed=5).gate_records(np.complex128)
+    more = W.brick(n, 20, seed=6).gate_records(np.complex128)
+    x = rand_state(n, np.complex128, 9)
+    want = oracle.apply(x.copy(), recs)
+    H = ising(n)
+    want_h = oracle.observable_apply(want, H.matrix_free_terms())
+    sa, sb = torch.cuda.Stream(), torch.cuda.Stream()
+    with StateVector(n, np.complex128) as src, StateVector(n, np.complex128) as dst, \
+            StateVector(n, np.complex128) as hdst:
+        src.set_stream(sa.cuda_stream)
+        dst.set_stream(sb.cuda_stream)
+        hdst.set_stream(sb.cuda_stream)
+        src.upload(x)
+        src.apply(recs)            # queued on src's stream
+        dst.copy_from(src)         # on dst's stream, after src's queue
+        hdst.apply_observable(src, H)  # on src's stream, hdst's stream waits for it
+        src.apply(more)            # src's stream waits for the copy's read
+        assert np.array_equal(dst.download(), want)
+        assert np.max(np.abs(hdst.download() - want_h)) < 1e-12
+    torch.cuda.synchronize()

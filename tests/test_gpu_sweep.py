@@ -1,7 +1,11 @@
-"""The sweep timing command (python -m qclab_b200.sweep) on every engine."""
+"""The sweep timing command (python -m qclab_b200.sweep) on every engine:
+plan statistics, timings, and the swept state against the oracle."""
+import numpy as np
 import pytest
 
+import oracle
 from qclab_b200 import sweep
+from qclab_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
 
@@ -10,10 +14,17 @@ pytestmark = pytest.mark.gpu
                                           ("c64", 3), ("c64", 4)])
 def test_sweep_command(cuda, dtype, engine):
     out = sweep.main(["--qubits", "14", "--depth", "6", "--dtype", dtype, "--engine",
-                      str(engine), "--repeat", "1"])
+                      str(engine), "--repeat", "1"], keep_state=True)
     assert out["gates"] == 14 * 6 + sum(len(range(l % 2, 13, 2)) for l in range(6))
     assert out["stages"] >= 1 and out["passes"] >= out["stages"]
     assert len(out["ms"]) == 1 and out["gates_per_s"] > 0
+    # the swept state: the same seeded circuit through the C oracle in FP64
+    recs = W.brick(14, 6, seed=3).gate_records(np.complex128)
+    want = np.zeros(1 << 14, dtype=np.complex128)
+    want[0] = 1
+    oracle.apply(want, recs)
+    tol = 1e-12 if dtype == "c128" else 2e-5
+    assert np.max(np.abs(out["state"].astype(np.complex128) - want)) < tol
 
 
 def test_sweep_adjoint_and_batch(cuda):
