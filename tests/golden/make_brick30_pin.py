@@ -38,6 +38,7 @@ HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parent.parent))
 
 import oracle  # noqa: E402
+from qclab_b200 import util  # noqa: E402
 from qclab_b200 import workloads as W  # noqa: E402
 
 QUBITS, DEPTH, SEED = 30, 200, 2024
@@ -57,19 +58,12 @@ def sample_indices(n: int = QUBITS) -> np.ndarray:
 
 
 def state_summary(state: np.ndarray) -> dict:
-    """Digest, norm, samples and block profile of one final state."""
-    h = hashlib.sha256()
-    chunk = 1 << 24
-    for s in range(0, state.size, chunk):
-        h.update(memoryview(state[s:s + chunk]).cast("B"))
-    p = np.empty(BLOCKS, dtype=np.float64)
-    bs = state.size // BLOCKS
-    for b in range(BLOCKS):
-        seg = state[b * bs:(b + 1) * bs]
-        p[b] = float(np.sum(seg.real.astype(np.float64) ** 2 + seg.imag.astype(np.float64) ** 2))
-    idx = sample_indices(int(state.size).bit_length() - 1)
-    return {"sha256": h.hexdigest(), "norm2": float(p.sum()), "idx": idx,
-            "amp": state[idx].copy(), "block_p": p}
+    """Digest, norm, samples and block profile of one final state (the same
+    routine the GPU side runs on its downloaded chunks)."""
+    n = int(state.size).bit_length() - 1
+    chunk = 1 << min(n, 26)
+    return util.state_summary((state[s:s + chunk] for s in range(0, state.size, chunk)), n,
+                              sample_indices(n), BLOCKS)
 
 
 def main() -> None:
