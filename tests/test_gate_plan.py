@@ -1,0 +1,78 @@
+"""The gate-specialised engine's plan on the host (no GPU): gate records are
+lowered, planned and factored exactly as the GPU executor does it, applied
+by the host mirror of the device ops (tests/cpp/gate_plan_test.cpp) and
+compared with the C oracle within 1e-12.  Covers every gate class, every
+op, offsets, 4- and 5-bit register passes and tile/low-bit shapes, and the
+brick circuit of the benchmark."""
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from qclab_b200 import workloads as W
+
+ROOT = Path(__file__).resolve().parent.parent
+CSRC = ROOT / "qclab_b200" / "csrc"
+
+
+@pytest.fixture(scope="module")
+def binary(tmp_path_factory):
+    out = tmp_path_factory.mktemp("gp") / "gate_plan_test"
+    r = subprocess.run(["g++", "-O2", "-std=c++17", f"-I{ROOT / 'include'}", f"-I{CSRC}",
+                        str(ROOT / "tests" / "cpp" / "gate_plan_test.cpp"), str(CSRC / "plan.cpp"),
+                        "-o", str(out)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+    return out
+
+
+def run_plan(binary, tmp_path, n, recs, x, R, m, low, op="N", offset=0):
+    rp, sp, op_ = tmp_path / "r.bin", tmp_path / "s.bin", tmp_path / "o.bin"
+    rp.write_bytes(np.ascontiguousarray(recs).tobytes())
+    sp.write_bytes(np.ascontiguousarray(x, dtype=np.complex128).tobytes())
+    r = subprocess.run([str(binary), str(n), str(R), str(m), str(low), op, str(offset), str(rp),
+                        str(sp), str(op_)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    stages, passes, ops = (int(v) for v in r.stdout.split())
+    return np.frombuffer(op_.read_bytes(), dtype=np.complex128), stages, passes, ops
+
+
+def rand_state(n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    return x / np.linalg.norm(x)
+
+
+@pytest.mark.parametrize("R,m,low", [(4, 8, 2), (4, 10, 3), (5, 9, 3), (5, 11, 4), (4, 6, 1)])
+@pytest.mark.parametrize("op", ["N", "T", "C"])
+def test_mixed_circuits_match_oracle(binary, tmp_path, R, m, low, op):
+    n = 11
+    recs = W.random_mixed(n, 400, seed=R * 100 + m).gate_records(np.complex128)
+    x = rand_state(n, m)
+    want = oracle.apply(x.copy(), recs, op)
+    got, stages, passes, ops = run_plan(binary, tmp_path, n, recs, x, R, m, low, op)
+    assert stages >= 1 and passes >= stages
+    assert np.max(np.abs(got - want)) < 1e-12
+
+
+def test_offset_and_small_register(binary, tmp_path):
+    n = 9
+    recs = W.random_mixed(6, 200, seed=3).gate_records(np.complex128)
+    x = rand_state(n, 1)
+    want = oracle.apply(x.copy(), recs, "N", 3)
+    got, *_ = run_plan(binary, tmp_path, n, recs, x, 4, 7, 2, "N", 3)
+    assert np.max(np.abs(got - want)) < 1e-12
+
+
+@pytest.mark.parametrize("R", [4, 5])
+def test_brick_circuit(binary, tmp_path, R):
+    n = 14
+    recs = W.brick(n, 30, seed=2024).gate_records(np.complex128)
+    x = np.zeros(1 << n, dtype=np.complex128)
+    x[0] = 1
+    want = oracle.apply(x.copy(), recs)
+    got, stages, passes, ops = run_plan(binary, tmp_path, n, recs, x, R, 12, 2)
+    assert np.max(np.abs(got - want)) < 1e-12
+    # every gate is one op, plus one scale op per stage
+    assert ops <= len(recs) + stages
