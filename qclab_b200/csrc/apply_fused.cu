@@ -30,6 +30,39 @@
 namespace qsv {
 
 static thread_local std::vector<float> g_stage_ms;
+
+StageTimer::StageTimer(bool on, size_t nstages, cudaStream_t stream)
+    : on_(on), stream_(stream), ev_(on ? nstages + 1 : 0, nullptr) {}
+
+StageTimer::~StageTimer() {
+  for (cudaEvent_t e : ev_)
+    if (e) cudaEventDestroy(e);
+}
+
+qsv_status StageTimer::start() {
+  if (!on_) return QSV_SUCCESS;
+  for (auto& e : ev_)
+    if (qsv_status st = cuda_status(cudaEventCreate(&e), "cudaEventCreate")) return st;
+  return cuda_status(cudaEventRecord(ev_[0], stream_), "cudaEventRecord");
+}
+
+qsv_status StageTimer::mark(size_t stage) {
+  if (!on_) return QSV_SUCCESS;
+  return cuda_status(cudaEventRecord(ev_[stage + 1], stream_), "cudaEventRecord");
+}
+
+qsv_status StageTimer::finish() {
+  if (!on_) return QSV_SUCCESS;
+  if (qsv_status st = cuda_status(cudaEventSynchronize(ev_.back()), "stage timing synchronize"))
+    return st;
+  g_stage_ms.clear();
+  for (size_t i = 0; i + 1 < ev_.size(); ++i) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev_[i], ev_[i + 1]);
+    g_stage_ms.push_back(ms);
+  }
+  return QSV_SUCCESS;
+}
 static std::atomic<bool> g_tc_used{false};  // a tcgen05 sweep was launched
 
 namespace fx {
@@ -990,6 +1023,19 @@ int dmma_tile_bits(int n, const qsv_fuse_opts* opts) {
   return md >= 7 ? md : -1;
 }
 
+// The gate engine runs when asked for (engine 5).
+bool use_gate_engine(const qsv_fuse_opts* opts) { return opts && opts->engine == 5; }
+
+// Tile bits of the gate engine: the requested (or default) size, at most 14
+// and n, with the tile and a plan in shared memory; -1 if too small.
+template <typename V>
+int gate_tile_bits(int n, const qsv_fuse_opts* opts) {
+  int m = (opts && opts->tile_bits > 0) ? opts->tile_bits : default_tile_bits(sizeof(V), 1);
+  m = std::min(std::min(m, 14), n);
+  while (m > 1 && (size_t(1) << m) * sizeof(V) + 16384 > 200 * 1024) --m;
+  return m >= gate_pass_bits(sizeof(V), opts) + 1 ? m : -1;
+}
+
 int dmma_pass_bits(int m) { return (QSV_DMMA_BITS == 3 && m >= 8) ? 3 : 2; }
 
 // The tensor-core engine's plan.  A dense pass costs the same whatever it
@@ -1177,8 +1223,18 @@ qsv_status execute_typed(const ExecArgs& x) {
                      (reinterpret_cast<uintptr_t>(x.v0) % 16 == 0) &&
                      (x.nv == 1 || reinterpret_cast<uintptr_t>(x.v1) % 16 == 0);
 
-  // complex single-vector sweeps run on the tensor-core engine unless the
-  // caller asks for sparse passes; tiles need at least one 128-amplitude chunk
+  // complex single-vector sweeps: the gate engine when selected, else the
+  // tensor-core engine unless the caller asks for sparse passes; tiles need
+  // at least one 128-amplitude chunk
+  if constexpr (Elem<V>::cplx) {
+    if (x.nv == 1 && x.nslots == 0 && use_gate_engine(opts)) {
+      const int mg = gate_tile_bits<V>(n, opts);
+      if (mg > 0) {
+        const qsv_status st = execute_gates<V>(x, mg, std::min(low, mg), max_gates, vec16);
+        if (st != QSV_ERROR_NOT_SUPPORTED) return st;
+      }
+    }
+  }
   if (x.nv == 1 && x.nslots == 0) {
     const int md = dmma_tile_bits<V>(n, opts);
     if (md > 0) {
@@ -1347,6 +1403,22 @@ namespace {
 template <typename V>
 qsv_status plan_counts(const std::vector<Lowered>& low, int n, const qsv_fuse_opts* opts,
                        std::vector<int>* ops, std::vector<int>* passes) {
+  if constexpr (Elem<V>::cplx) {
+    const int mg = use_gate_engine(opts) ? gate_tile_bits<V>(n, opts) : -1;
+    if (mg > 0) {
+      const int lowb = std::min((opts && opts->low_bits > 0) ? opts->low_bits
+                                                             : default_low_bits(sizeof(V)), mg);
+      const int max_gates = (opts && opts->max_stage_gates > 0) ? opts->max_stage_gates : 256;
+      std::vector<int> o, p;
+      const qsv_status st = gate_plan_counts(low, n, mg, lowb, opts, max_gates, sizeof(V), &o, &p);
+      if (st == QSV_SUCCESS) {
+        *ops = o;
+        *passes = p;
+        return st;
+      }
+      if (st != QSV_ERROR_NOT_SUPPORTED) return st;
+    }
+  }
   const int md = dmma_tile_bits<V>(n, opts);
   if (md > 0) {  // the tensor-core engine's plan (its ops are the passes' matrices)
     const int lowb = std::min((opts && opts->low_bits > 0) ? opts->low_bits : default_low_bits(sizeof(V)), md);

@@ -1,0 +1,415 @@
+// Gate-specialised stage kernel for single-vector complex sweeps
+// (complex<double> and complex<float> states).
+//
+// Same stage/tile structure as the other fused engines (plan.hpp,
+// stage_exec.cuh): one 2^m-amplitude tile per CTA is copied into shared
+// memory (16-byte cp.async, XOR-swizzled layout), the stage's register
+// passes run on it, and it is written back.  What differs is the op
+// application (gate_plan.hpp): every op is one case of a switch on a dense
+// code (kind x register positions, gate_cases.inc), so its register indices
+// are compile-time, and one-qubit gates are factored to two multiply-adds
+// per amplitude component with their scalar folded into the stage's kappa.
+// A brick layer's RotationX/RotationY/Hadamard therefore costs 2 FMAs or
+// adds per component, RotationZ a complex multiply on half the amplitudes,
+// CNOT register moves and CZ sign flips -- against 16 FMAs per component for
+// a dense 3-bit pass of the tensor-core engine.
+//
+// Arithmetic is FMA-contracted in the element's precision (the fused path's
+// contract: within 1e-12 of the reference-exact path for complex<double>).
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "fused.hpp"
+#include "gate_plan.hpp"
+#include "stage_exec.cuh"
+#include "gate_cases.inc"
+
+namespace qsv {
+namespace gx {
+
+using fx::align16;
+using fx::copy_words;
+using fx::ins0;
+using fx::ld_pair;
+using fx::load_tile;
+using fx::phys;
+using fx::st_pair;
+using fx::store_tile;
+
+template <typename V> struct RealOf;
+template <> struct RealOf<double2> { using T = double; };
+template <> struct RealOf<float2> { using T = float; };
+
+template <typename V, typename T>
+__device__ __forceinline__ V mk(T a, T b) { return V{a, b}; }
+
+// ---- ops (positions compile-time; x: the thread's N = 2^R registers) --------
+template <int K, int P, typename V, int N>
+__device__ __forceinline__ void op1(V (&x)[N], const V* __restrict__ c) {
+  using T = typename RealOf<V>::T;
+  constexpr int M = 1 << P;
+  T ca = T(0), cb = T(0);
+  V c0{};
+  if constexpr (K == G_SHEAR || K == G_SHEARO || K == G_ISHEAR || K == G_ISHEARO) {
+    const V cc = c[0];
+    ca = cc.x;
+    cb = cc.y;
+  } else if constexpr (K == G_PHASE) {
+    c0 = c[0];
+  }
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    if (j & M) continue;
+    const V a = x[j], b = x[j | M];
+    if constexpr (K == G_H) {
+      x[j] = mk<V>(a.x + b.x, a.y + b.y);
+      x[j | M] = mk<V>(a.x - b.x, a.y - b.y);
+    } else if constexpr (K == G_SHEAR) {
+      x[j] = mk<V>(fma(ca, b.x, a.x), fma(ca, b.y, a.y));
+      x[j | M] = mk<V>(fma(cb, a.x, b.x), fma(cb, a.y, b.y));
+    } else if constexpr (K == G_SHEARO) {
+      x[j] = mk<V>(fma(ca, a.x, -b.x), fma(ca, a.y, -b.y));
+      x[j | M] = mk<V>(fma(cb, b.x, a.x), fma(cb, b.y, a.y));
+    } else if constexpr (K == G_ISHEAR) {  // (a + i ca b, i cb a + b)
+      x[j] = mk<V>(fma(-ca, b.y, a.x), fma(ca, b.x, a.y));
+      x[j | M] = mk<V>(fma(-cb, a.y, b.x), fma(cb, a.x, b.y));
+    } else if constexpr (K == G_ISHEARO) {  // (ca a - i b, -i a + cb b)
+      x[j] = mk<V>(fma(ca, a.x, b.y), fma(ca, a.y, -b.x));
+      x[j | M] = mk<V>(fma(cb, b.x, a.y), fma(cb, b.y, -a.x));
+    } else if constexpr (K == G_PHASE) {
+      x[j | M] = fmul(c0, b);
+    } else if constexpr (K == G_GEN2) {  // coefficients read at their point of use
+      x[j] = fmac(fmul(fx::ld_use(c), a), fx::ld_use(c + 1), b);
+      x[j | M] = fmac(fmul(fx::ld_use(c + 2), a), fx::ld_use(c + 3), b);
+    } else if constexpr (K == G_REAL2) {  // c[0] = (m00, m01), c[1] = (m10, m11)
+      const V r0 = fx::ld_use(c), r1 = fx::ld_use(c + 1);
+      x[j] = mk<V>(fma(r0.x, a.x, r0.y * b.x), fma(r0.x, a.y, r0.y * b.y));
+      x[j | M] = mk<V>(fma(r1.x, a.x, r1.y * b.x), fma(r1.x, a.y, r1.y * b.y));
+    } else if constexpr (K == G_X) {
+      x[j] = b;
+      x[j | M] = a;
+    } else if constexpr (K == G_Z) {
+      x[j | M] = mk<V>(-b.x, -b.y);
+    }
+  }
+}
+
+template <int K, int Pt, int Pc, int CV, typename V, int N>
+__device__ __forceinline__ void op2(V (&x)[N], const V* __restrict__ c) {
+  constexpr int MT = 1 << Pt, MC = 1 << Pc;
+  V c0{};
+  if constexpr (K == G_CPH) c0 = c[0];
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    if ((j & MT) || (((j & MC) ? 1 : 0) != CV)) continue;
+    const V a = x[j], b = x[j | MT];
+    if constexpr (K == G_CX) {
+      x[j] = b;
+      x[j | MT] = a;
+    } else if constexpr (K == G_CGEN2) {  // coefficients read at their point of use
+      x[j] = fmac(fmul(fx::ld_use(c), a), fx::ld_use(c + 1), b);
+      x[j | MT] = fmac(fmul(fx::ld_use(c + 2), a), fx::ld_use(c + 3), b);
+    } else if constexpr (K == G_CNEG) {
+      x[j | MT] = mk<V>(-b.x, -b.y);
+    } else if constexpr (K == G_CPH) {
+      x[j | MT] = fmul(c0, b);
+    }
+  }
+}
+
+template <int K, int P0, int P1, typename V, int N>
+__device__ __forceinline__ void op4(V (&x)[N], const V* __restrict__ c) {
+  constexpr int M0 = 1 << P0, M1 = 1 << P1;
+  V z{};
+  if constexpr (K == G_ISWAP) z = c[0];
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    if ((j & M0) || (j & M1)) continue;
+    if constexpr (K == G_SWAP || K == G_ISWAP) {
+      const V s1 = x[j | M0], s2 = x[j | M1];
+      x[j | M0] = (K == G_ISWAP) ? fmul(z, s2) : s2;
+      x[j | M1] = (K == G_ISWAP) ? fmul(z, s1) : s1;
+    } else {
+      // coefficients read at their point of use, so the 16 of them never
+      // occupy registers together
+      const V s0 = x[j], s1 = x[j | M0], s2 = x[j | M1], s3 = x[j | M0 | M1];
+      V y[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        y[r] = fmac(fmac(fmac(fmul(fx::ld_use(c + 4 * r), s0), fx::ld_use(c + 4 * r + 1), s1),
+                         fx::ld_use(c + 4 * r + 2), s2),
+                    fx::ld_use(c + 4 * r + 3), s3);
+      x[j] = y[0]; x[j | M0] = y[1]; x[j | M1] = y[2]; x[j | M0 | M1] = y[3];
+    }
+  }
+}
+
+template <typename V, int N>
+__device__ __forceinline__ void op_scale(V (&x)[N], const V* __restrict__ c) {
+  const V z = c[0];
+#pragma unroll
+  for (int j = 0; j < N; ++j) x[j] = fmul(z, x[j]);
+}
+
+// One op word: code | coefficient index << kCodeBits (gate_plan.hpp).
+template <typename V, int R>
+__device__ __forceinline__ void apply_word(V (&x)[1 << R], uint32_t w, const V* __restrict__ cf) {
+  const V* __restrict__ c = cf + (w >> kCodeBits);
+  const uint32_t code = w & ((1u << kCodeBits) - 1u);
+  if constexpr (R == 4) {
+    switch (code) {
+      QSV_GX_CASES_4
+      default: break;
+    }
+  } else {
+    static_assert(R == 5, "register passes of 4 or 5 bits");
+    switch (code) {
+      QSV_GX_CASES_5
+      default: break;
+    }
+  }
+}
+
+// ---- the stage kernel --------------------------------------------------------
+// Device form of a register pass: its R tile bits, its ops, and
+// boff[k] = phys(1 << pos[k]), so that the swizzled shared-memory index of
+// register j is phys(tb) ^ XOR_{k in j} boff[k] (the swizzle is linear over
+// GF(2) in the index bits).
+struct GxPassDev {
+  int8_t pos[8];
+  int32_t op0;
+  int32_t nops;
+  uint32_t boff[8];
+};
+static_assert(sizeof(GxPassDev) == 48, "GxPassDev layout");
+
+struct GxArgs {
+  TileArgs ta;
+  int npasses, nops, ncoef;
+  const GxPassDev* passes;
+  const uint32_t* ops;
+  const void* coefs;  // V
+  int vec16;
+};
+
+template <int R>
+__device__ __forceinline__ uint32_t reg_off(uint32_t ptb, const uint32_t (&boff)[R], int j) {
+  uint32_t o = ptb;
+#pragma unroll
+  for (int k = 0; k < R; ++k)
+    if ((j >> k) & 1) o ^= boff[k];
+  return o;
+}
+
+template <typename V, int R, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_gates(V* __restrict__ v0, GxArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t size = 1u << a.ta.m;
+  V* t0 = reinterpret_cast<V*>(smem_raw);
+  // the stage's plan, copied once per CTA: passes | op words | coefficients
+  unsigned char* pp = smem_raw + size_t(size) * sizeof(V);
+  unsigned char* po = pp + align16(size_t(a.npasses) * sizeof(GxPassDev));
+  unsigned char* pc = po + align16(size_t(a.nops) * sizeof(uint32_t));
+  copy_words(pp, a.passes, size_t(a.npasses) * sizeof(GxPassDev));
+  copy_words(po, a.ops, size_t(a.nops) * sizeof(uint32_t));
+  copy_words(pc, a.coefs, size_t(a.ncoef) * sizeof(V));
+  const GxPassDev* passes = reinterpret_cast<const GxPassDev*>(pp);
+  const uint32_t* ops = reinterpret_cast<const uint32_t*>(po);
+  const V* coefs = reinterpret_cast<const V*>(pc);
+  const uint64_t base = tile_base(a.ta, blockIdx.x);
+  load_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
+  __syncthreads();
+  constexpr int N = 1 << R;
+  const uint32_t ngroups = size >> R;
+  for (int pi = 0; pi < a.npasses; ++pi) {
+    const GxPassDev& P = passes[pi];
+    uint32_t boff[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) boff[k] = P.boff[k];
+    const int op0 = P.op0, nops = P.nops;
+    // 8-byte elements with tile bit 0 in the pass: registers 2i and 2i+1 are
+    // the two halves of one 16-byte unit, moved as one access
+    const bool pairs = sizeof(V) == 8 && P.pos[0] == 0;
+    for (uint32_t g = threadIdx.x; g < ngroups; g += blockDim.x) {
+      uint32_t tb = g;
+#pragma unroll
+      for (int k = 0; k < R; ++k) tb = ins0(tb, P.pos[k]);
+      const uint32_t ptb = phys<V>(tb);
+      V x[N];
+      // register j sits at ptb ^ XOR_{k in j} boff[k]; recomputed for the
+      // store rather than held across the ops
+      if (pairs) {
+#pragma unroll
+        for (int j = 0; j < N; j += 2) ld_pair(t0 + reg_off<R>(ptb, boff, j), x[j], x[j + 1]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < N; ++j) x[j] = t0[reg_off<R>(ptb, boff, j)];
+      }
+      for (int o = 0; o < nops; ++o) apply_word<V, R>(x, ops[op0 + o], coefs);
+      if (pairs) {
+#pragma unroll
+        for (int j = 0; j < N; j += 2) st_pair(t0 + reg_off<R>(ptb, boff, j), x[j], x[j + 1]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < N; ++j) t0[reg_off<R>(ptb, boff, j)] = x[j];
+      }
+    }
+    __syncthreads();
+  }
+  store_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
+}
+
+// Launch shapes.  A thread holds 2^R amplitudes (64 registers for
+// complex<double> with R = 4, whose op switch needs ~190 registers in all),
+// so complex<double> runs CTAs of 128 threads, two per SM (each thread takes
+// two register groups per pass of a 2^12 tile); complex<float> with R = 4
+// fits three 256-thread CTAs per SM, with R = 5 two 128-thread CTAs.
+template <typename V> struct GxKernels;
+template <> struct GxKernels<double2> {
+  static void* get(int R) { (void)R; return (void*)k_gates<double2, 4, 128, 2>; }
+  static int threads(int R) { (void)R; return 128; }
+};
+template <> struct GxKernels<float2> {
+  static void* get(int R) {
+    return R == 5 ? (void*)k_gates<float2, 5, 128, 2> : (void*)k_gates<float2, 4, 256, 3>;
+  }
+  static int threads(int R) { return R == 5 ? 128 : 256; }
+};
+
+template <typename V> V to_elem(cplx z);
+template <> double2 to_elem<double2>(cplx z) { return make_double2(z.real(), z.imag()); }
+template <> float2 to_elem<float2>(cplx z) {
+  return make_float2((float)z.real(), (float)z.imag());
+}
+
+constexpr size_t kGxPlanCap = 16384;  // a stage's plan bytes in shared memory (bound)
+
+template <typename V>
+size_t gx_plan_smem(size_t npasses, size_t nops, size_t ncoef) {
+  return align16(npasses * sizeof(GxPassDev)) + align16(nops * sizeof(uint32_t)) +
+         align16(ncoef * sizeof(V));
+}
+
+}  // namespace gx
+
+int gate_pass_bits(size_t elem_bytes, const qsv_fuse_opts* opts) {
+  // complex<double> passes hold 4 bits (5 would not fit the registers)
+  return (elem_bytes < 16 && opts && opts->reg_bits == 5) ? 5 : 4;
+}
+
+namespace {
+
+qsv_status pack_gates_for(const std::vector<Lowered>& items, int n, int m, int low, int R,
+                          int max_gates, size_t elem_bytes, gx::GxPlan* plan) {
+  if (!gx::pack_gate_plan(items, n, m, low, R, max_gates, gx::kGxPlanCap, elem_bytes, plan))
+    return QSV_ERROR_NOT_SUPPORTED;
+  return QSV_SUCCESS;
+}
+
+}  // namespace
+
+template <typename V>
+qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool vec16) {
+  using namespace gx;
+  qsv_state_s* s = x.s;
+  const int n = s->n;
+  const int R = gate_pass_bits(sizeof(V), x.opts);
+  if (m < R + 1) return QSV_ERROR_NOT_SUPPORTED;
+  GxPlan plan;
+  if (qsv_status st = pack_gates_for(*x.items, n, m, low, R, max_gates, sizeof(V), &plan))
+    return st;
+  if (plan.stages.empty()) return QSV_SUCCESS;
+  std::vector<GxPassDev> dpass(plan.passes.size());
+  std::vector<uint64_t> runoff;
+  std::vector<size_t> run0;
+  for (const GxStage& gs : plan.stages) {
+    for (size_t pi = gs.pass0; pi < gs.pass0 + gs.npasses; ++pi) {
+      const GxPass& gp = plan.passes[pi];
+      GxPassDev& d = dpass[pi];
+      d = GxPassDev{};
+      for (int k = 0; k < 8; ++k) d.pos[k] = gp.pos[k];
+      d.op0 = gp.op0;
+      d.nops = gp.nops;
+      for (int k = 0; k < R; ++k) d.boff[k] = fx::phys_host(1u << gp.pos[k], fx::Units<V>::per);
+    }
+    run0.push_back(runoff.size());
+    tile_runoffs(gs.bits, gs.m, low, &runoff);
+  }
+  auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
+  const size_t pass_bytes = dpass.size() * sizeof(GxPassDev);
+  const size_t op_off = align(pass_bytes);
+  const size_t coef_off = align(op_off + plan.ops.size() * sizeof(uint32_t));
+  const size_t run_off = align(coef_off + plan.coefs.size() * sizeof(V));
+  const size_t total = run_off + runoff.size() * sizeof(uint64_t);
+  std::vector<unsigned char> host(total);
+  std::memcpy(host.data(), dpass.data(), pass_bytes);
+  std::memcpy(host.data() + op_off, plan.ops.data(), plan.ops.size() * sizeof(uint32_t));
+  V* hc = reinterpret_cast<V*>(host.data() + coef_off);
+  for (size_t i = 0; i < plan.coefs.size(); ++i) hc[i] = to_elem<V>(plan.coefs[i]);
+  std::memcpy(host.data() + run_off, runoff.data(), runoff.size() * sizeof(uint64_t));
+  if (qsv_status st = ensure_scratch(s, total)) return st;
+  unsigned char* dev = static_cast<unsigned char*>(s->scratch);
+  if (qsv_status st = cuda_status(cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice,
+                                                  s->stream), "gate plan upload"))
+    return st;
+  void* kern = GxKernels<V>::get(R);
+  if (qsv_status st = cuda_status(cudaFuncSetAttribute(kern,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       200 * 1024), "gate stage shared-memory attribute"))
+    return st;
+  const uint64_t ntiles = 1ull << (n - m);
+  if (x.ntiles_out) *x.ntiles_out = ntiles;
+  const unsigned threads =
+      (unsigned)std::min<uint64_t>((uint64_t)GxKernels<V>::threads(R), 1ull << (m - R));
+  StageTimer timer(x.opts && x.opts->profile, plan.stages.size(), s->stream);
+  if (qsv_status st = timer.start()) return st;
+  V* p0 = static_cast<V*>(x.v0);
+  for (size_t si = 0; si < plan.stages.size(); ++si) {
+    const GxStage& gs = plan.stages[si];
+    GxArgs a;
+    a.ta.n = n;
+    a.ta.m = gs.m;
+    a.ta.low = low;
+    for (int j = 0; j < 64; ++j) a.ta.bits[j] = (int8_t)gs.bits[j];
+    a.ta.runoff = reinterpret_cast<const uint64_t*>(dev + run_off) + run0[si];
+    a.npasses = (int)gs.npasses;
+    a.nops = (int)gs.nops;
+    a.ncoef = (int)gs.ncoef;
+    a.passes = reinterpret_cast<const GxPassDev*>(dev) + gs.pass0;
+    a.ops = reinterpret_cast<const uint32_t*>(dev + op_off) + gs.op0;
+    a.coefs = dev + coef_off + gs.coef0 * sizeof(V);
+    a.vec16 = vec16 ? 1 : 0;
+    const size_t smem =
+        (size_t(1) << gs.m) * sizeof(V) + gx_plan_smem<V>(gs.npasses, gs.nops, gs.ncoef);
+    if (smem > 200 * 1024)
+      return fail(QSV_ERROR_SIZE, "gate stage needs %zu bytes of shared memory", smem);
+    void* args[] = {&p0, &a};
+    if (qsv_status st = cuda_status(cudaLaunchKernel(kern, dim3((unsigned)ntiles), dim3(threads),
+                                                     args, smem, s->stream),
+                                    "gate stage launch"))
+      return st;
+    count_launch();
+    if (qsv_status st = timer.mark(si)) return st;
+  }
+  return timer.finish();
+}
+
+template qsv_status execute_gates<double2>(const ExecArgs&, int, int, int, bool);
+template qsv_status execute_gates<float2>(const ExecArgs&, int, int, int, bool);
+
+qsv_status gate_plan_counts(const std::vector<Lowered>& items, int n, int m, int low,
+                            const qsv_fuse_opts* opts, int max_gates, size_t elem_bytes,
+                            std::vector<int>* ops, std::vector<int>* passes) {
+  gx::GxPlan plan;
+  if (qsv_status st = pack_gates_for(items, n, m, low, gate_pass_bits(elem_bytes, opts),
+                                     max_gates, elem_bytes, &plan))
+    return st;
+  for (const gx::GxStage& gs : plan.stages) {
+    ops->push_back((int)gs.nops);
+    passes->push_back((int)gs.npasses);
+  }
+  return QSV_SUCCESS;
+}
+
+}  // namespace qsv

@@ -23,6 +23,38 @@ struct ExecArgs {
 };
 
 int default_tile_bits(size_t elem_bytes, int nv);
+
+// Per-stage CUDA-event timing of a fused sweep (qsv_fuse_opts.profile): an
+// event before the first stage and after each one, on the sweep's stream;
+// finish() waits for the last event and stores the durations for
+// qsv_last_stage_times.  Does nothing when off.
+class StageTimer {
+ public:
+  StageTimer(bool on, size_t nstages, cudaStream_t stream);
+  ~StageTimer();
+  qsv_status start();
+  qsv_status mark(size_t stage);
+  qsv_status finish();
+
+ private:
+  bool on_;
+  cudaStream_t stream_;
+  std::vector<cudaEvent_t> ev_;
+};
+
+// Single-vector sweep of a complex<double> / complex<float> state on the
+// gate-specialised engine (apply_gates.cu) with tiles of 2^m amplitudes;
+// QSV_ERROR_NOT_SUPPORTED, with nothing launched, when the items do not fit
+// it.
+template <typename V>
+qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool vec16);
+// Register bits of its passes: 4, or 5 for 8-byte elements with
+// qsv_fuse_opts.reg_bits = 5.
+int gate_pass_bits(size_t elem_bytes, const qsv_fuse_opts* opts);
+// Its plan statistics: ops and passes per stage.
+qsv_status gate_plan_counts(const std::vector<Lowered>& items, int n, int m, int low,
+                            const qsv_fuse_opts* opts, int max_gates, size_t elem_bytes,
+                            std::vector<int>* ops, std::vector<int>* passes);
 int default_low_bits(size_t elem_bytes);
 
 // Plans the items into stages and runs them.

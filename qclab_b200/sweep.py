@@ -11,7 +11,8 @@ the plan (``qsv_plan_passes``), the wall time of each sweep (host planning
 included, stream synchronised) and gates/s.  ``--engine`` is
 ``qsv_fuse_opts.engine``: 0 default (FP64 MMA), 1 sparse register passes,
 2 as 0, 3 tcgen05 TF32 for complex<float>, 4 mma.sync TF32 for
-complex<float>.
+complex<float>, 5 gate-specialised register passes (``--reg-bits`` 4, or 5
+for complex<float>).
 
 adjoint: energy and full gradient (``qsv_adjoint_gradient``) of the
 hardware-efficient ansatz ``workloads.hea(qubits, depth)`` for
@@ -48,6 +49,7 @@ def main(argv=None, keep_state: bool = False) -> dict:
     p.add_argument("--engine", type=int, default=0)
     p.add_argument("--tile-bits", type=int, default=0)
     p.add_argument("--low-bits", type=int, default=0)
+    p.add_argument("--reg-bits", type=int, default=0)
     p.add_argument("--repeat", type=int, default=2)
     p.add_argument("--workload", choices=["brick", "adjoint", "batch"], default="brick")
     p.add_argument("--circuits", type=int, default=512)
@@ -58,7 +60,8 @@ def main(argv=None, keep_state: bool = False) -> dict:
         return _batch(a)
     dt, code = DTYPES[a.dtype]
     recs = W.brick(a.qubits, a.depth, seed=a.seed).gate_records(dt)
-    opts = L.FuseOpts(engine=a.engine, tile_bits=a.tile_bits, low_bits=a.low_bits)
+    opts = L.FuseOpts(engine=a.engine, tile_bits=a.tile_bits, low_bits=a.low_bits,
+                      reg_bits=a.reg_bits)
     lib = L.load()
     arr, ptr, cnt = L.gate_array(recs)
     ns, npas, nops = C.c_int(), C.c_int(), C.c_int()

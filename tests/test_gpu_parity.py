@@ -85,9 +85,13 @@ def test_fused_matches_reference_within_tolerance(states, dtype):
         # engine 0 (tensor-core dense passes for complex states with tiles of
         # >= 7 bits, FP64 MMA), engine 1 (sparse register passes), engine 2
         # (as 0), engine 3 (complex<float> TF32 on tcgen05 for tiles of >= 10
-        # bits), engine 4 (complex<float> TF32 on mma.sync)
+        # bits), engine 4 (complex<float> TF32 on mma.sync), engine 5 (gate-
+        # specialised passes of 4 bits, or 5 for complex<float>)
         for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=2), L.FuseOpts(engine=3),
-                     L.FuseOpts(engine=4),
+                     L.FuseOpts(engine=4), L.FuseOpts(engine=5),
+                     L.FuseOpts(engine=5, reg_bits=5),
+                     L.FuseOpts(engine=5, tile_bits=6, low_bits=1),
+                     L.FuseOpts(engine=5, tile_bits=12, low_bits=5, max_stage_gates=3),
                      L.FuseOpts(tile_bits=10, low_bits=3, engine=3),
                      L.FuseOpts(tile_bits=4, low_bits=2),
                      L.FuseOpts(tile_bits=6, low_bits=1), L.FuseOpts(tile_bits=7, low_bits=2),
@@ -112,7 +116,7 @@ def test_random_mixed_large(states, dtype, n):
         y = run_gpu(states, n, dtype, recs, op, 0, x)
         assert np.array_equal(y, ref)
         for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=2), L.FuseOpts(engine=3),
-                     L.FuseOpts(engine=4)):
+                     L.FuseOpts(engine=4), L.FuseOpts(engine=5), L.FuseOpts(engine=5, reg_bits=5)):
             yf = run_gpu(states, n, dtype, recs, op, 0, x, fused=True, opts=opts)
             assert np.max(np.abs(yf - ref)) <= tol(dtype), (op, opts and opts.engine)
 
@@ -149,7 +153,8 @@ def test_complex_float_fused_keeps_the_norm(states):
     x = np.zeros(1 << n, dtype=np.complex128)
     x[0] = 1
     ref = run_gpu(states, n, np.complex128, r128, "N", 0, x, fused=True)
-    for opts, bound in ((None, 1e-6), (L.FuseOpts(engine=4), 1e-3)):
+    for opts, bound in ((None, 1e-6), (L.FuseOpts(engine=4), 1e-3), (L.FuseOpts(engine=5), 1e-6),
+                        (L.FuseOpts(engine=5, reg_bits=5), 1e-6)):
         y = run_gpu(states, n, np.complex64, r128, "N", 0, x.astype(np.complex64), fused=True,
                     opts=opts).astype(np.complex128)
         infid = 1.0 - abs(np.vdot(ref, y)) ** 2
@@ -168,7 +173,8 @@ def test_fused_small_states_and_empty_lists(states, dtype):
         x = (rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)).astype(dtype)
         x /= np.linalg.norm(x)
         ref = oracle.apply(x.copy(), recs, "N")
-        for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=3), L.FuseOpts(engine=4)):
+        for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=3), L.FuseOpts(engine=4),
+                     L.FuseOpts(engine=5), L.FuseOpts(engine=5, reg_bits=5)):
             y = run_gpu(states, n, dtype, recs, "N", 0, x, fused=True, opts=opts)
             assert np.max(np.abs(y - ref)) <= tol(dtype), (n, opts and opts.engine)
         for fused in (False, True):

@@ -10,7 +10,8 @@ from qclab_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("dtype,engine", [("c128", 0), ("c128", 1), ("c64", 0), ("c64", 2),
+@pytest.mark.parametrize("dtype,engine", [("c128", 0), ("c128", 1), ("c128", 5), ("c64", 5),
+                                          ("c64", 0), ("c64", 2),
                                           ("c64", 3), ("c64", 4)])
 def test_sweep_command(cuda, dtype, engine):
     out = sweep.main(["--qubits", "14", "--depth", "6", "--dtype", dtype, "--engine",
