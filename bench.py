@@ -51,20 +51,22 @@ def parse_args():
     p.add_argument("--parity-layers", type=int, default=10)
     p.add_argument("--no-extras", action="store_true",
                    help="skip the adjoint (24q) and precision (32q) measurements")
-    p.add_argument("--ps-params", type=int, default=24,
-                   help="parameters timed for the parameter-shift baseline")
+    p.add_argument("--ps-params", type=int, default=0,
+                   help="angles timed for the parameter-shift baseline (0 = all 576)")
     return p.parse_args()
 
 
-def adjoint_extra(torch, stream, ps_params):
+def adjoint_extra(torch, stream, ps_params, fd_params=48, fd_h=1e-5):
     """Adjoint gradient on the 24-qubit hardware-efficient ansatz (12 layers of
     RotationY/RotationZ on every qubit + a CNOT ladder: 852 gates, 576
-    angles), complex<double>, H = sum Z_i Z_{i+1} + 0.5 sum X_i.  The GPU
-    parameter-shift baseline is timed on `ps_params` angles and extrapolated
-    to all 576 (each angle costs the same two simulations)."""
+    angles), complex<double>, H = sum Z_i Z_{i+1} + 0.5 sum X_i, checked
+    against the GPU parameter-shift gradient on every angle (`ps_params` = 0;
+    a positive count times that many evenly spaced angles and extrapolates)
+    and central finite differences (h = `fd_h`) on `fd_params` seeded angles."""
     from qclab_b200 import StateVector
     from qclab_b200 import workloads as W
-    from qclab_b200.gradients import adjoint_gradient, parameter_shift_gradient
+    from qclab_b200.gradients import (adjoint_gradient, finite_difference_gradient,
+                                      parameter_shift_gradient)
     from qclab_b200.observable import ising
     n = 24
     recs = W.hea(n, 12, seed=7).gate_records(np.complex128, number_params=True)
@@ -85,7 +87,8 @@ def adjoint_extra(torch, stream, ps_params):
         torch.cuda.synchronize()
         adj_ms = a.elapsed_time(b) / reps
         s.set_basis(0)
-        subset = set(range(0, nparams, max(1, nparams // ps_params)))
+        subset = (set(range(nparams)) if ps_params <= 0
+                  else set(range(0, nparams, max(1, nparams // ps_params))))
         parameter_shift_gradient(s, recs, H, params={0})  # warm-up
         torch.cuda.synchronize()
         a.record(stream)
@@ -93,74 +96,112 @@ def adjoint_extra(torch, stream, ps_params):
         b.record(stream)
         torch.cuda.synchronize()
         ps_ms = a.elapsed_time(b) * nparams / len(subset)
+        rng = np.random.default_rng(24)
+        fd_set = set(int(v) for v in rng.choice(nparams, size=min(fd_params, nparams),
+                                                replace=False))
+        fd = finite_difference_gradient(s, recs, H, h=fd_h, params=fd_set)
     err = float(max(abs(g[p] - ps[p]) for p in subset))
+    fd_err = float(max(abs(g[p] - fd[p]) for p in fd_set))
     return {"workload": "hea24_12layers_c128_ising", "gates": len(recs), "params": nparams,
             "energy": e, "adjoint_ms": adj_ms, "grads_per_s": 1e3 / adj_ms,
-            "param_shift_ms_extrapolated": ps_ms, "param_shift_params_timed": len(subset),
-            "speedup_vs_param_shift": ps_ms / adj_ms, "max_abs_grad_diff_vs_param_shift": err}
+            "param_shift_ms": ps_ms, "param_shift_params_timed": len(subset),
+            "param_shift_extrapolated": len(subset) < nparams,
+            "speedup_vs_param_shift": ps_ms / adj_ms,
+            "max_abs_grad_diff_vs_param_shift": err,
+            "central_fd": {"h": fd_h, "params": len(fd_set), "seed": 24,
+                           "max_abs_grad_diff_vs_adjoint": fd_err},
+            "max_abs_grad": float(np.max(np.abs(g)))}
+
+
+def plan_counts(n, code, recs, opts=None):
+    """(stages, register passes) of the fused plan qsv_apply_fused would run."""
+    from qclab_b200 import _lib as L
+    lib = L.load()
+    st_, ps_, op_ = C.c_int(), C.c_int(), C.c_int()
+    L.check(lib.qsv_plan_passes(n, code, C.c_void_p(recs.ctypes.data), len(recs), b"N", 0,
+                                C.byref(opts) if opts is not None else None, C.byref(st_),
+                                C.byref(ps_), C.byref(op_)), "qsv_plan_passes")
+    return st_.value, ps_.value
 
 
 def precision_extra(torch, stream, n=32, depth=100, seed=11):
     """Precision study: the brick generator at n qubits, depth `depth`, run in
     complex<float> and complex<double> (fused), compared in FP64.  Both runs
-    take the circuit's gate parameters in double (the fused path multiplies
-    gates out in FP64 for either state type), so the difference is the
-    state's precision alone."""
+    take the circuit's gate parameters in double, so the difference is the
+    state's precision (and the engine's arithmetic) alone.  Each
+    complex<float> engine gets its HBM roofline (stages x one read + one
+    write of the 32 GiB state over its time), and the plain unfused
+    complex<double> path (qsv_apply) is timed on the circuit's first layer
+    at the same size."""
     from qclab_b200 import StateVector
+    from qclab_b200 import _lib as L
     from qclab_b200 import workloads as W
     from qclab_b200.observable import Observable
     circ = W.brick(n, depth, seed=seed)
     r128 = circ.gate_records(np.complex128)
-    r64 = r128  # the same double-precision parameters for the complex<float> state
     zz = Observable(n).add(1.0, {0: "Z", 1: "Z"})
+    peak, peak_kind = peaks()
     out = {"workload": f"brick{n}_depth{depth}", "gates": len(r128)}
+
+    def timed(fn):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1])
+
     with StateVector(n, np.complex128) as d, StateVector(n, np.complex64) as f:
         d.set_stream(stream.cuda_stream)
         f.set_stream(stream.cuda_stream)
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        torch.cuda.synchronize()
-        ev[0].record(stream)
-        f.apply(r64, "N", 0, fused=True)
-        ev[1].record(stream)
-        d.apply(r128, "N", 0, fused=True)
-        ev[2].record(stream)
-        torch.cuda.synchronize()
-        ip_raw, maxabs_raw = f.compare(d)
-        norm_f = f.normalize()   # FP64 norm, removes any float norm drift
-        norm_d = d.normalize()
-        ip, maxabs = f.compare(d)
-        zf, zd = f.expectation(zz), d.expectation(zz)
-        c64_ms, c128_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
-        # the opt-in TF32 engine (mma.sync, three-term split) on the same circuit
-        from qclab_b200 import _lib as L
-        et = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        f.set_basis(0)
-        torch.cuda.synchronize()
-        et[0].record(stream)
-        f.apply(r64, "N", 0, fused=True, opts=L.FuseOpts(engine=4))
-        et[1].record(stream)
-        torch.cuda.synchronize()
-        ip_tf32, mx_tf32 = f.compare(d)
-        norm_tf32 = f.normalize()
-        ip_tf32n, _ = f.compare(d)
-        tf32 = {"engine": 4, "c64_ms": et[0].elapsed_time(et[1]),
-                "c64_gates_per_s": len(r64) / (et[0].elapsed_time(et[1]) / 1e3),
-                "infidelity": 1.0 - abs(ip_tf32) ** 2, "max_abs_error": mx_tf32,
-                "norm2_c64": norm_tf32,
-                "infidelity_after_fp64_renormalisation": 1.0 - abs(ip_tf32n) ** 2}
-        out.update({"c64_ms": c64_ms, "c128_ms": c128_ms,
-                    "c64_gates_per_s": len(r64) / (c64_ms / 1e3),
-                    "c128_gates_per_s": len(r128) / (c128_ms / 1e3),
-                    "infidelity": 1.0 - abs(ip_raw) ** 2, "max_abs_error": maxabs_raw,
-                    "infidelity_after_fp64_renormalisation": 1.0 - abs(ip) ** 2,
-                    "max_abs_error_after_fp64_renormalisation": maxabs,
-                    "zz01_c64": zf, "zz01_c128": zd, "zz01_error": abs(zf - zd),
-                    "norm2_c64": norm_f, "norm2_c128": norm_d,
-                    "c64_engine": "default: FP64 MMA passes, state rounded once per pass",
-                    "note": "infidelity = 1 - |<psi32|psi64>|^2 of the states as computed; "
-                            "renormalising a float state whose norm is within an ulp of 1 "
-                            "quantises the scale (a few 1e-8)",
-                    "tf32_engine": tf32})
+        c128_ms = timed(lambda: d.apply(r128, "N", 0, fused=True))
+        d_norm2 = d.norm2()
+        zd = d.expectation(zz)
+        engines = [("default", None), ("gates_r4", L.FuseOpts(engine=5)),
+                   ("gates_r5", L.FuseOpts(engine=5, reg_bits=5)),
+                   ("tf32_mma_sync", L.FuseOpts(engine=4))]
+        runs = {}
+        for name, opts in engines:
+            f.set_basis(0)
+            f.apply(r128[:1], "N", 0, fused=True, opts=opts)  # loads the kernel
+            f.set_basis(0)
+            ms = timed(lambda: f.apply(r128, "N", 0, fused=True, opts=opts))
+            ip, maxabs = f.compare(d)
+            zf = f.expectation(zz)
+            nf = f.norm2()
+            stages, passes = plan_counts(n, L.C64, r128, opts)
+            achieved = stages * 2 * (1 << n) * 8 / (ms / 1e3) / 1e9
+            runs[name] = {"ms": ms, "gates_per_s": len(r128) / (ms / 1e3),
+                          "infidelity": 1.0 - abs(ip) ** 2, "max_abs_error": maxabs,
+                          "zz01_error": abs(zf - zd), "norm2_c64": nf,
+                          "stages": stages, "passes": passes,
+                          "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                                       "unit": "GB/s", "frac": achieved / peak,
+                                       "peak_source": f"{peak_kind} hbm_gbs"}}
+        # the plain unfused complex<double> path on the circuit's first layer
+        layer = r128[:W.brick_layer_sizes(n, 1)[0]]
+        d.set_basis(0)
+        d.apply(layer[:1], "N", 0, fused=False)
+        d.set_basis(0)
+        u_ms = timed(lambda: d.apply(layer, "N", 0, fused=False))
+        u_bytes = sum((2 if int(r["kind"]) in (L.HADAMARD, L.ROTATION_X, L.ROTATION_Y,
+                                                L.ROTATION_Z) else 1 if int(r["kind"]) == L.CX
+                       else 0.5) * (1 << n) * 16 for r in layer)
+        unfused = {"gates": len(layer), "ms": u_ms, "gates_per_s": len(layer) / (u_ms / 1e3),
+                   "hbm_gbs": u_bytes / (u_ms / 1e3) / 1e9, "path": "qsv_apply (bit-exact)"}
+    best = runs["default"]
+    out.update({"c64_ms": best["ms"], "c128_ms": c128_ms,
+                "c64_gates_per_s": best["gates_per_s"],
+                "c128_gates_per_s": len(r128) / (c128_ms / 1e3),
+                "infidelity": best["infidelity"], "max_abs_error": best["max_abs_error"],
+                "zz01_c128": zd, "zz01_error": best["zz01_error"],
+                "norm2_c64": best["norm2_c64"], "norm2_c128": d_norm2,
+                "roofline_c64": best["roofline"], "c64_engines": runs,
+                "unfused_c128_first_layer": unfused,
+                "c64_fused_vs_unfused_c128": best["gates_per_s"] / unfused["gates_per_s"],
+                "note": "infidelity = 1 - |<psi32|psi64>|^2 of the states as computed, "
+                        "without renormalisation; TF32 is opt-in (its accumulation truncates)"})
     return out
 
 
@@ -423,6 +464,53 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def full_size_parity(torch, stream, n, args, recs, sv):
+    """Parity of this step's fused complex<double> state `sv` (and of a fused
+    complex<float> sweep) against the reference-exact path; the latter is
+    checked against the committed summary of QCLAB++'s CPU simulate on the
+    same circuit (tests/golden/make_brick30_pin.py) when that fixture exists
+    for this workload."""
+    from qclab_b200 import StateVector
+    fix = ROOT / "tests" / "golden" / f"brick{n}_d{args.depth}_s{args.seed}_c128.npz"
+    want = dict(np.load(fix)) if fix.exists() else None
+    sub = recs if want is not None else recs[:sum(
+        n + len(range(l % 2, n - 1, 2)) for l in range(max(args.parity_layers, 1)))]
+    out = {"gates": len(sub)}
+    with StateVector(n, np.complex128) as ref:
+        ref.set_stream(stream.cuda_stream)
+        ref.apply(sub, "N", 0, fused=False)
+        if want is not None:
+            got = ref.summary(want["idx"])
+            bitwise = (got["sha256"] == str(want["sha256"]) and
+                       bool(np.array_equal(got["amp"], want["amp"])) and
+                       bool(np.array_equal(got["block_p"], want["block_p"])))
+            out.update({"against": "QCLAB++ QCircuit::simulate digest (SHA-256 of the final "
+                                   "state, samples, block profile)",
+                        "bitwise": bitwise, "sha256": got["sha256"],
+                        "reference_cpu_seconds": float(want["seconds"])})
+        else:
+            out.update({"against": "qsv_apply (bitwise equal to QCLAB++ CPU apply in tests)",
+                        "bitwise": None})
+        if len(sub) < len(recs):  # else `sv` holds the fused state of the whole circuit
+            fused = StateVector(n, np.complex128)
+            fused.set_stream(stream.cuda_stream)
+            fused.apply(sub, "N", 0, fused=True)
+        else:
+            fused = None
+        ip, maxabs = (fused or sv).compare(ref)
+        if fused is not None:
+            fused.close()
+        out["c128_fused"] = {"max_abs_error": maxabs, "infidelity": 1.0 - abs(ip) ** 2,
+                             "bound": 1e-12}
+        with StateVector(n, np.complex64) as f:
+            f.set_stream(stream.cuda_stream)
+            f.apply(sub, "N", 0, fused=True)
+            ip, maxabs = f.compare(ref)
+        out["c64_fused"] = {"max_abs_error": maxabs, "infidelity": 1.0 - abs(ip) ** 2,
+                            "bound": 1e-5}
+    return out
+
+
 def workload_config(args, ngates, world):
     return {"workload": f"brick{args.qubits}_depth{args.depth}_c128", "qubits": args.qubits,
             "depth": args.depth, "gates": ngates, "seed": args.seed,
@@ -552,22 +640,14 @@ def main():
         unf = {"gates": len(sub), "gates_per_s": len(sub) / (ums / 1e3),
                "hbm_gbs": unf_bytes / (ums / 1e3) / 1e9, "path": "qsv_apply (bit-exact)"}
 
-    # parity at full size: fused sweep vs the reference-exact per-gate path
-    # (bitwise equal to QCLAB++'s CPU apply in the tests) on the first layers
+    # parity at full size: the reference-exact path over the whole circuit,
+    # pinned to QCLAB++'s own simulate by the committed digest when this is
+    # the pinned workload (else over the first layers), then the fused
+    # complex<double> state (this step's result) and a fused complex<float>
+    # sweep compared with it
     parity = None
-    if args.parity_layers > 0 and world == 1:
-        k = sum(n + len(range(l % 2, n - 1, 2)) for l in range(args.parity_layers))
-        sub = recs[:k]
-        ref_state = StateVector(n, np.complex128)
-        ref_state.set_stream(stream.cuda_stream)
-        ref_state.apply(sub, "N", 0, fused=False)
-        sv.set_basis(0)
-        sv.apply(sub, "N", 0, fused=True)
-        ip, maxabs = sv.compare(ref_state)
-        ref_state.close()
-        parity = {"gates": k, "layers": args.parity_layers, "max_abs_error": maxabs,
-                  "infidelity": 1.0 - abs(ip) ** 2,
-                  "against": "qsv_apply (bitwise equal to QCLAB++ CPU apply in tests)"}
+    if args.parity_layers != 0 and world == 1:
+        parity = full_size_parity(torch, stream, n, args, recs, sv)
 
     # end to end through the C ABI with host buffers (copies inside the timed region)
     e2e = None

@@ -92,6 +92,28 @@ class StateVector:
     def copy_from(self, other: "StateVector") -> None:
         L.check(self._lib.qsv_copy(self._h, other._h), "qsv_copy")
 
+    def chunks(self, chunk_qubits: int = 26):
+        """Yields the state's elements as host arrays of 2^chunk_qubits
+        elements in index order (each downloaded through a non-owning view
+        of that part of the device array; one chunk of host memory at a
+        time)."""
+        self.synchronize()
+        k = min(chunk_qubits, self.nbQubits)
+        step = (1 << k) * self.numpy_dtype.itemsize
+        base = self.device_ptr()
+        for i in range(1 << (self.nbQubits - k)):
+            view = StateVector.wrap(base + i * step, k, self.numpy_dtype)
+            try:
+                yield view.download()
+            finally:
+                view.close()
+
+    def summary(self, idx, blocks: int = 256) -> dict:
+        """``util.state_summary`` of this state: SHA-256 of its bytes, FP64
+        norm^2, the amplitudes at ``idx`` and per-block probabilities."""
+        from .util import state_summary
+        return state_summary(self.chunks(), self.nbQubits, idx, blocks)
+
     def synchronize(self) -> None:
         L.check(self._lib.qsv_synchronize(self._h), "qsv_synchronize")
 
