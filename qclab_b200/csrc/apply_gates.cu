@@ -44,6 +44,82 @@ template <> struct RealOf<float2> { using T = float; };
 template <typename V, typename T>
 __device__ __forceinline__ V mk(T a, T b) { return V{a, b}; }
 
+// ---- in-place register primitives --------------------------------------------
+// Each updates its "+" operands in place with one inline-PTX block (temporaries
+// inside the block), so the amplitude registers keep their registers from op
+// to op: written as plain C++, the switch's cases each produced new values
+// that the compiler then copied back at the loop join, several moves per
+// amplitude per op.
+__device__ __forceinline__ void ip_h(double& a, double& b) {  // (a + b, a - b)
+  asm("{\n .reg .f64 t;\n add.rn.f64 t, %0, %1;\n sub.rn.f64 %1, %0, %1;\n mov.f64 %0, t;\n}"
+      : "+d"(a), "+d"(b));
+}
+__device__ __forceinline__ void ip_h(float& a, float& b) {
+  asm("{\n .reg .f32 t;\n add.rn.f32 t, %0, %1;\n sub.rn.f32 %1, %0, %1;\n mov.f32 %0, t;\n}"
+      : "+f"(a), "+f"(b));
+}
+// (a + p b, q a + b)
+__device__ __forceinline__ void ip_sh(double& a, double& b, double p, double q) {
+  asm("{\n .reg .f64 t;\n fma.rn.f64 t, %2, %1, %0;\n fma.rn.f64 %1, %3, %0, %1;\n"
+      " mov.f64 %0, t;\n}" : "+d"(a), "+d"(b) : "d"(p), "d"(q));
+}
+__device__ __forceinline__ void ip_sh(float& a, float& b, float p, float q) {
+  asm("{\n .reg .f32 t;\n fma.rn.f32 t, %2, %1, %0;\n fma.rn.f32 %1, %3, %0, %1;\n"
+      " mov.f32 %0, t;\n}" : "+f"(a), "+f"(b) : "f"(p), "f"(q));
+}
+// (p a - b, a + q b)
+__device__ __forceinline__ void ip_sho(double& a, double& b, double p, double q) {
+  asm("{\n .reg .f64 t, u;\n neg.f64 u, %1;\n fma.rn.f64 t, %2, %0, u;\n"
+      " fma.rn.f64 %1, %3, %1, %0;\n mov.f64 %0, t;\n}" : "+d"(a), "+d"(b) : "d"(p), "d"(q));
+}
+__device__ __forceinline__ void ip_sho(float& a, float& b, float p, float q) {
+  asm("{\n .reg .f32 t, u;\n neg.f32 u, %1;\n fma.rn.f32 t, %2, %0, u;\n"
+      " fma.rn.f32 %1, %3, %1, %0;\n mov.f32 %0, t;\n}" : "+f"(a), "+f"(b) : "f"(p), "f"(q));
+}
+// (p a + b, q b - a)
+__device__ __forceinline__ void ip_shop(double& a, double& b, double p, double q) {
+  asm("{\n .reg .f64 t, u;\n fma.rn.f64 t, %2, %0, %1;\n neg.f64 u, %0;\n"
+      " fma.rn.f64 %1, %3, %1, u;\n mov.f64 %0, t;\n}" : "+d"(a), "+d"(b) : "d"(p), "d"(q));
+}
+__device__ __forceinline__ void ip_shop(float& a, float& b, float p, float q) {
+  asm("{\n .reg .f32 t, u;\n fma.rn.f32 t, %2, %0, %1;\n neg.f32 u, %0;\n"
+      " fma.rn.f32 %1, %3, %1, u;\n mov.f32 %0, t;\n}" : "+f"(a), "+f"(b) : "f"(p), "f"(q));
+}
+// (re, im) *= (zr + i zi)
+__device__ __forceinline__ void ip_cmul(double& re, double& im, double zr, double zi) {
+  asm("{\n .reg .f64 t, u;\n mul.rn.f64 t, %3, %1;\n mul.rn.f64 u, %3, %0;\n neg.f64 t, t;\n"
+      " fma.rn.f64 %0, %2, %0, t;\n fma.rn.f64 %1, %2, %1, u;\n}"
+      : "+d"(re), "+d"(im) : "d"(zr), "d"(zi));
+}
+__device__ __forceinline__ void ip_cmul(float& re, float& im, float zr, float zi) {
+  asm("{\n .reg .f32 t, u;\n mul.rn.f32 t, %3, %1;\n mul.rn.f32 u, %3, %0;\n neg.f32 t, t;\n"
+      " fma.rn.f32 %0, %2, %0, t;\n fma.rn.f32 %1, %2, %1, u;\n}"
+      : "+f"(re), "+f"(im) : "f"(zr), "f"(zi));
+}
+__device__ __forceinline__ void ip_swap(double& a, double& b) {
+  asm("{\n .reg .f64 t;\n mov.f64 t, %0;\n mov.f64 %0, %1;\n mov.f64 %1, t;\n}"
+      : "+d"(a), "+d"(b));
+}
+__device__ __forceinline__ void ip_swap(float& a, float& b) {
+  asm("{\n .reg .f32 t;\n mov.f32 t, %0;\n mov.f32 %0, %1;\n mov.f32 %1, t;\n}"
+      : "+f"(a), "+f"(b));
+}
+__device__ __forceinline__ void ip_neg(double& a) { asm("neg.f64 %0, %0;" : "+d"(a)); }
+__device__ __forceinline__ void ip_neg(float& a) { asm("neg.f32 %0, %0;" : "+f"(a)); }
+
+template <typename V>
+__device__ __forceinline__ void ip_cmulv(V& x, const V& z) { ip_cmul(x.x, x.y, z.x, z.y); }
+template <typename V>
+__device__ __forceinline__ void ip_swapv(V& a, V& b) {
+  ip_swap(a.x, b.x);
+  ip_swap(a.y, b.y);
+}
+template <typename V>
+__device__ __forceinline__ void ip_negv(V& a) {
+  ip_neg(a.x);
+  ip_neg(a.y);
+}
+
 // ---- ops (positions compile-time; x: the thread's N = 2^R registers) --------
 template <int K, int P, typename V, int N>
 __device__ __forceinline__ void op1(V (&x)[N], const V* __restrict__ c) {
@@ -61,36 +137,42 @@ __device__ __forceinline__ void op1(V (&x)[N], const V* __restrict__ c) {
 #pragma unroll
   for (int j = 0; j < N; ++j) {
     if (j & M) continue;
-    const V a = x[j], b = x[j | M];
+    V& a = x[j];
+    V& b = x[j | M];
     if constexpr (K == G_H) {
-      x[j] = mk<V>(a.x + b.x, a.y + b.y);
-      x[j | M] = mk<V>(a.x - b.x, a.y - b.y);
+      ip_h(a.x, b.x);
+      ip_h(a.y, b.y);
     } else if constexpr (K == G_SHEAR) {
-      x[j] = mk<V>(fma(ca, b.x, a.x), fma(ca, b.y, a.y));
-      x[j | M] = mk<V>(fma(cb, a.x, b.x), fma(cb, a.y, b.y));
+      ip_sh(a.x, b.x, ca, cb);
+      ip_sh(a.y, b.y, ca, cb);
     } else if constexpr (K == G_SHEARO) {
-      x[j] = mk<V>(fma(ca, a.x, -b.x), fma(ca, a.y, -b.y));
-      x[j | M] = mk<V>(fma(cb, b.x, a.x), fma(cb, b.y, a.y));
-    } else if constexpr (K == G_ISHEAR) {  // (a + i ca b, i cb a + b)
-      x[j] = mk<V>(fma(-ca, b.y, a.x), fma(ca, b.x, a.y));
-      x[j | M] = mk<V>(fma(-cb, a.y, b.x), fma(cb, a.x, b.y));
-    } else if constexpr (K == G_ISHEARO) {  // (ca a - i b, -i a + cb b)
-      x[j] = mk<V>(fma(ca, a.x, b.y), fma(ca, a.y, -b.x));
-      x[j | M] = mk<V>(fma(cb, b.x, a.y), fma(cb, b.y, -a.x));
+      ip_sho(a.x, b.x, ca, cb);
+      ip_sho(a.y, b.y, ca, cb);
+    } else if constexpr (K == G_ISHEAR) {
+      // (a + i ca b, i cb a + b): shears of (a.re, b.im) and (a.im, b.re)
+      ip_sh(a.x, b.y, -ca, cb);
+      ip_sh(a.y, b.x, ca, -cb);
+    } else if constexpr (K == G_ISHEARO) {
+      // (ca a - i b, -i a + cb b)
+      ip_shop(a.x, b.y, ca, cb);
+      ip_sho(a.y, b.x, ca, cb);
     } else if constexpr (K == G_PHASE) {
-      x[j | M] = fmul(c0, b);
+      ip_cmulv(b, c0);
     } else if constexpr (K == G_GEN2) {  // coefficients read at their point of use
-      x[j] = fmac(fmul(fx::ld_use(c), a), fx::ld_use(c + 1), b);
-      x[j | M] = fmac(fmul(fx::ld_use(c + 2), a), fx::ld_use(c + 3), b);
+      const V y1 = fmac(fmul(fx::ld_use(c), a), fx::ld_use(c + 1), b);
+      const V y2 = fmac(fmul(fx::ld_use(c + 2), a), fx::ld_use(c + 3), b);
+      a = y1;
+      b = y2;
     } else if constexpr (K == G_REAL2) {  // c[0] = (m00, m01), c[1] = (m10, m11)
       const V r0 = fx::ld_use(c), r1 = fx::ld_use(c + 1);
-      x[j] = mk<V>(fma(r0.x, a.x, r0.y * b.x), fma(r0.x, a.y, r0.y * b.y));
-      x[j | M] = mk<V>(fma(r1.x, a.x, r1.y * b.x), fma(r1.x, a.y, r1.y * b.y));
+      const V y1 = mk<V>(fma(r0.x, a.x, r0.y * b.x), fma(r0.x, a.y, r0.y * b.y));
+      const V y2 = mk<V>(fma(r1.x, a.x, r1.y * b.x), fma(r1.x, a.y, r1.y * b.y));
+      a = y1;
+      b = y2;
     } else if constexpr (K == G_X) {
-      x[j] = b;
-      x[j | M] = a;
+      ip_swapv(a, b);
     } else if constexpr (K == G_Z) {
-      x[j | M] = mk<V>(-b.x, -b.y);
+      ip_negv(b);
     }
   }
 }
@@ -103,17 +185,19 @@ __device__ __forceinline__ void op2(V (&x)[N], const V* __restrict__ c) {
 #pragma unroll
   for (int j = 0; j < N; ++j) {
     if ((j & MT) || (((j & MC) ? 1 : 0) != CV)) continue;
-    const V a = x[j], b = x[j | MT];
+    V& a = x[j];
+    V& b = x[j | MT];
     if constexpr (K == G_CX) {
-      x[j] = b;
-      x[j | MT] = a;
+      ip_swapv(a, b);
     } else if constexpr (K == G_CGEN2) {  // coefficients read at their point of use
-      x[j] = fmac(fmul(fx::ld_use(c), a), fx::ld_use(c + 1), b);
-      x[j | MT] = fmac(fmul(fx::ld_use(c + 2), a), fx::ld_use(c + 3), b);
+      const V y1 = fmac(fmul(fx::ld_use(c), a), fx::ld_use(c + 1), b);
+      const V y2 = fmac(fmul(fx::ld_use(c + 2), a), fx::ld_use(c + 3), b);
+      a = y1;
+      b = y2;
     } else if constexpr (K == G_CNEG) {
-      x[j | MT] = mk<V>(-b.x, -b.y);
+      ip_negv(b);
     } else if constexpr (K == G_CPH) {
-      x[j | MT] = fmul(c0, b);
+      ip_cmulv(b, c0);
     }
   }
 }
@@ -127,9 +211,11 @@ __device__ __forceinline__ void op4(V (&x)[N], const V* __restrict__ c) {
   for (int j = 0; j < N; ++j) {
     if ((j & M0) || (j & M1)) continue;
     if constexpr (K == G_SWAP || K == G_ISWAP) {
-      const V s1 = x[j | M0], s2 = x[j | M1];
-      x[j | M0] = (K == G_ISWAP) ? fmul(z, s2) : s2;
-      x[j | M1] = (K == G_ISWAP) ? fmul(z, s1) : s1;
+      ip_swapv(x[j | M0], x[j | M1]);
+      if constexpr (K == G_ISWAP) {
+        ip_cmulv(x[j | M0], z);
+        ip_cmulv(x[j | M1], z);
+      }
     } else {
       // coefficients read at their point of use, so the 16 of them never
       // occupy registers together
@@ -149,7 +235,7 @@ template <typename V, int N>
 __device__ __forceinline__ void op_scale(V (&x)[N], const V* __restrict__ c) {
   const V z = c[0];
 #pragma unroll
-  for (int j = 0; j < N; ++j) x[j] = fmul(z, x[j]);
+  for (int j = 0; j < N; ++j) ip_cmulv(x[j], z);
 }
 
 // One op word: code | coefficient index << kCodeBits (gate_plan.hpp).
@@ -160,13 +246,13 @@ __device__ __forceinline__ void apply_word(V (&x)[1 << R], uint32_t w, const V* 
   if constexpr (R == 4) {
     switch (code) {
       QSV_GX_CASES_4
-      default: break;
+      default: __builtin_unreachable();
     }
   } else {
     static_assert(R == 5, "register passes of 4 or 5 bits");
     switch (code) {
       QSV_GX_CASES_5
-      default: break;
+      default: __builtin_unreachable();
     }
   }
 }
