@@ -30,7 +30,6 @@ namespace gx {
 
 using fx::align16;
 using fx::copy_words;
-using fx::ins0;
 using fx::ld_pair;
 using fx::load_tile;
 using fx::phys;
@@ -262,13 +261,16 @@ __device__ __forceinline__ void apply_word(V (&x)[1 << R], uint32_t w, const V* 
 // boff[k] = phys(1 << pos[k]), so that the swizzled shared-memory index of
 // register j is phys(tb) ^ XOR_{k in j} boff[k] (the swizzle is linear over
 // GF(2) in the index bits).
+// goff[k] = phys(1 << tile bit of group-index bit k) (lane_order), so the
+// group's base is XOR_{k in g} goff[k].
 struct GxPassDev {
   int8_t pos[8];
   int32_t op0;
   int32_t nops;
   uint32_t boff[8];
+  uint32_t goff[12];
 };
-static_assert(sizeof(GxPassDev) == 48, "GxPassDev layout");
+static_assert(sizeof(GxPassDev) == 96, "GxPassDev layout");
 
 struct GxArgs {
   TileArgs ta;
@@ -317,11 +319,11 @@ __global__ void __launch_bounds__(NT, MINB) k_gates(V* __restrict__ v0, GxArgs a
     // 8-byte elements with tile bit 0 in the pass: registers 2i and 2i+1 are
     // the two halves of one 16-byte unit, moved as one access
     const bool pairs = sizeof(V) == 8 && P.pos[0] == 0;
+    const int gbits = a.ta.m - R;
     for (uint32_t g = threadIdx.x; g < ngroups; g += blockDim.x) {
-      uint32_t tb = g;
-#pragma unroll
-      for (int k = 0; k < R; ++k) tb = ins0(tb, P.pos[k]);
-      const uint32_t ptb = phys<V>(tb);
+      uint32_t ptb = 0;
+      for (int k = 0; k < gbits; ++k)
+        if ((g >> k) & 1u) ptb ^= P.goff[k];
       V x[N];
       // register j sits at ptb ^ XOR_{k in j} boff[k]; recomputed for the
       // store rather than held across the ops
@@ -418,6 +420,12 @@ qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool 
       d.op0 = gp.op0;
       d.nops = gp.nops;
       for (int k = 0; k < R; ++k) d.boff[k] = fx::phys_host(1u << gp.pos[k], fx::Units<V>::per);
+      int order[32];
+      int pos[8];
+      for (int k = 0; k < 8; ++k) pos[k] = gp.pos[k];
+      const int ng = lane_order(pos, R, gs.m, sizeof(V), order);
+      if (ng > 12) return fail(QSV_ERROR_SIZE, "gate stage of %d tile bits", gs.m);
+      for (int k = 0; k < ng; ++k) d.goff[k] = fx::phys_host(1u << order[k], fx::Units<V>::per);
     }
     run0.push_back(runoff.size());
     tile_runoffs(gs.bits, gs.m, low, &runoff);

@@ -305,6 +305,46 @@ inline void host_apply_op(cplx* x, int R, uint32_t word, const cplx* c) {
   for (int j = 0; j < N; ++j) x[j] *= c[0];  // scale
 }
 
+// ---- lane order ----------------------------------------------------------------
+// The tile bits that a pass's register-group index g spreads over (all
+// tile bits outside the pass), lowest g bit first, chosen so that the lanes
+// of one shared-memory wavefront hit distinct banks.  With the XOR swizzle
+// of stage_exec.cuh (16-byte unit u -> u ^ ((u>>3 ^ u>>6 ^ u>>9 ^ u>>12) & 7)),
+// tile bit b of a 16-byte element lands on 16-byte slot bit b mod 3 of the
+// 128-byte row, and of an 8-byte element (two per unit) on slot bit
+// (b - 1) mod 3, bit 0 selecting the half.  A wavefront serves 8 lanes of
+// 16-byte accesses (complex<double>, or complex<float> pairs when tile bit 0
+// is a pass bit) or 16 lanes of 8-byte accesses: their 3 (or 4) lowest g
+// bits should map to tile bits whose slot bits are distinct.
+inline int lane_order(const int* pos, int R, int m, size_t elem_bytes, int* order) {
+  uint32_t pass = 0;
+  for (int k = 0; k < R; ++k) pass |= 1u << pos[k];
+  std::vector<int> rest;
+  for (int b = 0; b < m; ++b)
+    if (!((pass >> b) & 1u)) rest.push_back(b);
+  const bool pairs = elem_bytes == 8 && (pass & 1u);
+  auto slot = [&](int b) { return elem_bytes >= 16 ? b % 3 : (b - 1) % 3; };
+  std::vector<int> first;
+  if (elem_bytes == 8 && !pairs && !rest.empty() && rest[0] == 0) first.push_back(0);
+  bool used[3] = {false, false, false};
+  for (int b : rest) {
+    if (b == 0 && elem_bytes == 8) continue;
+    const int sl = slot(b);
+    if (!used[sl]) {
+      used[sl] = true;
+      first.push_back(b);
+    }
+  }
+  int k = 0;
+  for (int b : first) order[k++] = b;
+  for (int b : rest) {
+    bool taken = false;
+    for (int f : first) taken = taken || (f == b);
+    if (!taken) order[k++] = b;
+  }
+  return k;
+}
+
 // ---- packing -----------------------------------------------------------------
 // Plans `gates` (single-vector items) for an n-qubit state with tiles of 2^m
 // amplitudes (`low` contiguous low bits) and register passes of R bits.
