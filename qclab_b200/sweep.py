@@ -21,6 +21,15 @@ H = sum Z_i Z_i+1 + 0.5 sum X_i; prints the time per gradient.
 batch: ``--circuits`` ansatz circuits of 8..18 qubits and 4..16 layers in one
 persistent launch (``qsv_batch_run``, default tile shape); prints the time
 per batch.
+
+kernels: one launch of every reference-exact per-gate kernel shape (pair,
+controlled pair and quad at register and lane bits, half-state and
+quarter-state phase scales, SWAP/iSWAP) and of the FP64 reductions (norm,
+inner product, expectation of the Ising H, state comparison) on a
+``--qubits`` complex<double> state; prints each one's best time over
+``--repeat`` launches and its achieved GB/s from the bytes the reference's
+loop touches (apply.hpp:259-371: 2 N s for pair and quad gates, N s for
+controlled pairs, half scales and swaps, N s / 2 for controlled scales).
 """
 from __future__ import annotations
 
@@ -51,13 +60,16 @@ def main(argv=None, keep_state: bool = False) -> dict:
     p.add_argument("--low-bits", type=int, default=0)
     p.add_argument("--reg-bits", type=int, default=0)
     p.add_argument("--repeat", type=int, default=2)
-    p.add_argument("--workload", choices=["brick", "adjoint", "batch"], default="brick")
+    p.add_argument("--workload", choices=["brick", "adjoint", "batch", "kernels"],
+                   default="brick")
     p.add_argument("--circuits", type=int, default=512)
     a = p.parse_args(argv)
     if a.workload == "adjoint":
         return _adjoint(a)
     if a.workload == "batch":
         return _batch(a)
+    if a.workload == "kernels":
+        return _kernels(a)
     dt, code = DTYPES[a.dtype]
     recs = W.brick(a.qubits, a.depth, seed=a.seed).gate_records(dt)
     opts = L.FuseOpts(engine=a.engine, tile_bits=a.tile_bits, low_bits=a.low_bits,
@@ -135,6 +147,63 @@ def _batch(a) -> dict:
             b.run()
             b.results()
         out["ms"] = _timed(run, a.repeat)
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def _kernels(a) -> dict:
+    from . import gates as G
+    from .circuit import QCircuit
+    from .observable import ising
+    n = a.qubits
+    N = 1 << n
+    s16 = N * 16
+    hi, lo = 0, n - 1  # qubit 0 is the top index bit (register kernels), n-1 bit 0 (lanes)
+    cases = [
+        ("k_pair_reg  Hadamard(top)", [G.Hadamard(hi)], 2 * s16),
+        ("k_pair_lane Hadamard(bit 0)", [G.Hadamard(lo)], 2 * s16),
+        ("k_pair_reg  CNOT(top)", [G.CNOT(hi, hi + 1)], s16),
+        ("k_pair_lane CNOT(bit 0)", [G.CNOT(lo - 1, lo)], s16),
+        ("k_scale     PauliZ (half)", [G.PauliZ(3)], s16),
+        ("k_scale     CZ (quarter)", [G.CZ(2, 3)], s16 // 2),
+        ("k_quad_reg2 RotationXX(top)", [G.RotationXX(hi, hi + 1, 0.3)], 2 * s16),
+        ("k_quad_reg1 RotationXX(reg, lane)", [G.RotationXX(n - 6, lo, 0.3)], 2 * s16),
+        ("k_quad_lane RotationXX(lanes)", [G.RotationXX(lo - 2, lo, 0.3)], 2 * s16),
+        ("k_swap_reg2 SWAP(top)", [G.SWAP(hi, hi + 1)], s16),
+        ("k_swap_reg1 iSWAP(reg, lane)", [G.iSWAP(n - 6, lo)], s16),
+        ("k_swap_lane SWAP(lanes)", [G.SWAP(lo - 2, lo)], s16),
+    ]
+    out = {"workload": "kernels", "qubits": n, "dtype": "c128", "kernels": {}}
+    H = ising(n)
+
+    def best(fn):
+        fn()
+        st.synchronize()
+        ms = []
+        for _ in range(max(1, a.repeat)):
+            t = time.perf_counter()
+            fn()
+            st.synchronize()
+            ms.append((time.perf_counter() - t) * 1e3)
+        return min(ms)
+
+    with StateVector(n, np.complex128) as st, StateVector(n, np.complex128) as other:
+        st.set_basis(0)
+        for name, gl, nbytes in cases:
+            c = QCircuit(n)
+            for g in gl:
+                c.push_back(g)
+            recs = c.gate_records(np.complex128)
+            ms = best(lambda: st.apply(recs, "N", 0, fused=False))
+            out["kernels"][name] = {"ms": round(ms, 4), "gbs": nbytes / (ms / 1e3) / 1e9}
+        reds = [("k_norm2 (norm)", lambda: st.norm2(), s16),
+                ("k_inner (inner product)", lambda: st.inner(other), 2 * s16),
+                ("k_compare (state comparison)", lambda: st.compare(other), 2 * s16),
+                ("k_expect* (Ising H, tiled groups)", lambda: st.expectation(H), None)]
+        for name, fn, nbytes in reds:
+            ms = best(fn)
+            out["kernels"][name] = {"ms": round(ms, 4),
+                                    "gbs": (nbytes / (ms / 1e3) / 1e9) if nbytes else None}
     print(json.dumps(out), flush=True)
     return out
 

@@ -34,3 +34,9 @@ def test_sweep_adjoint_and_batch(cuda):
     assert -20.0 < out["energy"] < 20.0
     out = sweep.main(["--workload", "batch", "--circuits", "16", "--dtype", "c64", "--repeat", "1"])
     assert out["circuits"] == 16 and out["gates"] > 0 and len(out["ms"]) == 1
+
+
+def test_sweep_kernels_workload(cuda):
+    out = sweep.main(["--workload", "kernels", "--qubits", "12", "--repeat", "1"])
+    assert len(out["kernels"]) == 16
+    assert all(v["ms"] > 0 for v in out["kernels"].values())
