@@ -169,7 +169,9 @@ typedef struct qsv_fuse_opts {
                         mma.sync.  The TF32 engines are faster but their
                         FP32 accumulation truncates: the norm shrinks by
                         about 1e-7 per pass.                               */
-  int reserved[2];
+  int ctas_per_sm;   /* engine 5: resident CTAs per SM the stage kernel is
+                        built for (0 = default; 2 or 3)                    */
+  int reserved;
 } qsv_fuse_opts;
 
 /* Fused path: the gate list is planned into stages; each stage streams the

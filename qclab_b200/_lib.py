@@ -52,7 +52,7 @@ class FuseOpts(C.Structure):
     """``qsv_fuse_opts``."""
     _fields_ = [("tile_bits", C.c_int), ("low_bits", C.c_int), ("reg_bits", C.c_int),
                 ("max_stage_gates", C.c_int), ("profile", C.c_int), ("engine", C.c_int),
-                ("reserved", C.c_int * 2)]
+                ("ctas_per_sm", C.c_int), ("reserved", C.c_int)]
 
 
 class BatchOpts(C.Structure):

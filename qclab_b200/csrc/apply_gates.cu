@@ -350,17 +350,23 @@ __global__ void __launch_bounds__(NT, MINB) k_gates(V* __restrict__ v0, GxArgs a
 
 // Launch shapes.  A thread holds 2^R amplitudes (64 registers for
 // complex<double> with R = 4, whose op switch needs ~190 registers in all),
-// so complex<double> runs CTAs of 128 threads, two per SM (each thread takes
-// two register groups per pass of a 2^12 tile); complex<float> with R = 4
-// fits three 256-thread CTAs per SM, with R = 5 two 128-thread CTAs.
+// so complex<double> runs CTAs of 128 threads, two per SM by default (three
+// with qsv_fuse_opts.ctas_per_sm = 3, at 168 registers); complex<float>
+// with R = 4 runs 256-thread CTAs, three per SM (two on request), with
+// R = 5 two 128-thread CTAs.  Each thread takes ngroups / threads register
+// groups per pass.
 template <typename V> struct GxKernels;
 template <> struct GxKernels<double2> {
-  static void* get(int R) { (void)R; return (void*)k_gates<double2, 4, 128, 2>; }
+  static void* get(int R, int ctas) {
+    (void)R;
+    return ctas == 3 ? (void*)k_gates<double2, 4, 128, 3> : (void*)k_gates<double2, 4, 128, 2>;
+  }
   static int threads(int R) { (void)R; return 128; }
 };
 template <> struct GxKernels<float2> {
-  static void* get(int R) {
-    return R == 5 ? (void*)k_gates<float2, 5, 128, 2> : (void*)k_gates<float2, 4, 256, 3>;
+  static void* get(int R, int ctas) {
+    if (R == 5) return (void*)k_gates<float2, 5, 128, 2>;
+    return ctas == 2 ? (void*)k_gates<float2, 4, 256, 2> : (void*)k_gates<float2, 4, 256, 3>;
   }
   static int threads(int R) { return R == 5 ? 128 : 256; }
 };
@@ -447,7 +453,7 @@ qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool 
   if (qsv_status st = cuda_status(cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice,
                                                   s->stream), "gate plan upload"))
     return st;
-  void* kern = GxKernels<V>::get(R);
+  void* kern = GxKernels<V>::get(R, x.opts ? x.opts->ctas_per_sm : 0);
   if (qsv_status st = cuda_status(cudaFuncSetAttribute(kern,
                                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                        200 * 1024), "gate stage shared-memory attribute"))

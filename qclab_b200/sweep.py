@@ -59,6 +59,7 @@ def main(argv=None, keep_state: bool = False) -> dict:
     p.add_argument("--tile-bits", type=int, default=0)
     p.add_argument("--low-bits", type=int, default=0)
     p.add_argument("--reg-bits", type=int, default=0)
+    p.add_argument("--ctas-per-sm", type=int, default=0)
     p.add_argument("--repeat", type=int, default=2)
     p.add_argument("--workload", choices=["brick", "adjoint", "batch", "kernels"],
                    default="brick")
@@ -73,7 +74,7 @@ def main(argv=None, keep_state: bool = False) -> dict:
     dt, code = DTYPES[a.dtype]
     recs = W.brick(a.qubits, a.depth, seed=a.seed).gate_records(dt)
     opts = L.FuseOpts(engine=a.engine, tile_bits=a.tile_bits, low_bits=a.low_bits,
-                      reg_bits=a.reg_bits)
+                      reg_bits=a.reg_bits, ctas_per_sm=a.ctas_per_sm)
     lib = L.load()
     arr, ptr, cnt = L.gate_array(recs)
     ns, npas, nops = C.c_int(), C.c_int(), C.c_int()
