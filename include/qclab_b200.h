@@ -279,9 +279,12 @@ qsv_status qsv_adjoint_gradient(qsv_state state, const qsv_gate* gates,
  * Many independent circuits, each with its own qubit count (5..30), gate
  * list and Pauli-sum observable: energy E_c = <psi_c|H_c|psi_c> from |0...0>
  * and the full adjoint gradient dE_c/dtheta_p of every circuit, computed by
- * ONE persistent kernel launch (a CTA per circuit at a time, largest
- * circuits first; circuits whose two work vectors fit a CTA's shared memory
- * never touch HBM) that qsv_batch_run can capture in a CUDA graph.
+ * ONE persistent kernel launch (largest circuits first; a circuit whose two
+ * work vectors fit a CTA's shared memory runs on one CTA and never touches
+ * HBM, a larger one on a team of CTAs that share its tiles stage by stage)
+ * that qsv_batch_run can capture in a CUDA graph.  Team barriers wait a
+ * bounded time; if one gives up, qsv_batch_results returns
+ * QSV_ERROR_TIMEOUT.
  *   gates + gate_offsets[c..c+1]     : circuit c's records (param >= 0 marks
  *                                      a trainable angle, < nParams[c])
  *   paulis/coefs + term_offsets[c..] : circuit c's terms (nbQubits[c] chars
@@ -292,7 +295,9 @@ typedef struct qsv_batch_opts {
   int tile_bits;     /* 2^m amplitudes per shared-memory tile (0 = default) */
   int low_bits;      /* contiguous low bits of a tile (0 = default)          */
   int ctas_per_sm;   /* cap on resident CTAs per SM (0 = occupancy limit)   */
-  int reserved[5];
+  int max_team;      /* most CTAs sharing one circuit larger than a tile
+                        (0 = 16; 1 = one CTA per circuit)                    */
+  int reserved[4];
 } qsv_batch_opts;
 qsv_status qsv_batch_create(qsv_dtype dtype, int nCircuits, const int* nbQubits,
                             const qsv_gate* gates, const size_t* gate_offsets,

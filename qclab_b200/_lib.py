@@ -58,7 +58,7 @@ class FuseOpts(C.Structure):
 class BatchOpts(C.Structure):
     """``qsv_batch_opts``."""
     _fields_ = [("tile_bits", C.c_int), ("low_bits", C.c_int), ("ctas_per_sm", C.c_int),
-                ("reserved", C.c_int * 5)]
+                ("max_team", C.c_int), ("reserved", C.c_int * 4)]
 
 
 GATE_DTYPE = np.dtype([

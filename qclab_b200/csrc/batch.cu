@@ -3,8 +3,13 @@
 // full adjoint gradient of every circuit, in ONE persistent kernel launch
 // captured in a CUDA graph.
 //
-// Every CTA pulls circuit indices from an atomic work counter (largest
-// circuits first) and runs a whole circuit by itself:
+// Every CTA pulls job indices from an atomic work counter (largest
+// circuits first).  A circuit that fits one tile runs on one CTA; a larger
+// one is split into a team of up to 16 consecutive jobs whose CTAs share its
+// tiles stage by stage, meeting at a team barrier (a counter in global
+// memory, bounded waits) between stages, so a few large circuits no longer
+// hold single CTAs long after the rest of the batch is done.  Each circuit
+// runs
 //   forward fused stages on psi  ->  lambda = H psi and E = <psi|lambda>
 //   ->  backward fused stages on (psi, lambda) with in-tile gradient terms.
 // A circuit whose two vectors fit in the CTA's shared memory (n <= m) never
@@ -40,6 +45,12 @@ struct qsv_batch_s {
   double* results = nullptr;  // [ncirc energies][grads] (device)
   size_t nresults = 0;
   unsigned* counter = nullptr;
+  unsigned* team_sync = nullptr;  // inside the results allocation
+  double* team_part = nullptr;
+  unsigned* error = nullptr;
+  size_t zero_bytes = 0;          // results + team state, zeroed before every launch
+  int njobs = 0;                  // job entries (a team counts once per member)
+  int nteams = 0;
   std::vector<size_t> grad_off;  // per circuit, into the gradient part
   std::vector<int> nparams;
   cudaGraph_t graph = nullptr;
@@ -80,7 +91,10 @@ struct BJob {
   int32_t fwd0, nfwd, bwd0, nbwd;   // stage ranges
   int32_t grp0, ngrp;               // term-group range
   int32_t circ;                     // circuit index (results)
+  int32_t team, rank, team_id;      // team size (1: one CTA), this job's rank, team index
+  int32_t nparams;
   int64_t grad_off;                 // into results (after the energies)
+  int64_t part_off;                 // team: its partial sums in BArgs.team_part
 };
 
 struct BArgs {
@@ -98,9 +112,40 @@ struct BArgs {
   size_t work_stride;    // elements per CTA slot (2 vectors)
   double* results;       // [ncirc] energies, then gradients
   unsigned* counter;
+  unsigned* team_sync;   // per team: [arrivals, 1 + blockIdx of rank 0, -, -]; then the error flag
+  double* team_part;     // per team: energies[team], then gradients[team][nparams]
+  unsigned* error;       // set when a team barrier gave up waiting
   int vec16;
   int tile_elems;        // 2^M: the shared-memory tiles hold 2 x tile_elems elements
 };
+
+// Spins of a team barrier before it gives up (with __nanosleep(100) each,
+// tens of seconds): the persistent grid is resident and teams are handed
+// out in order, so every member arrives; the limit only bounds a broken run.
+constexpr unsigned kTeamSpinLimit = 1u << 28;
+
+// Team barrier: all T members arrive, then each waits for the k-th round
+// (arrivals >= T (k + 1)).  Global writes before it are visible after it.
+__device__ __forceinline__ void team_barrier(unsigned* arrive, unsigned target, unsigned* error) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(arrive, 1u);
+    unsigned spins = 0;
+    while (true) {
+      unsigned v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(arrive) : "memory");
+      if (v >= target) break;
+      if (++spins > kTeamSpinLimit) {
+        atomicOr(error, 1u);
+        break;
+      }
+      __nanosleep(100);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
 
 template <typename V>
 __device__ __forceinline__ TileArgs stage_tile(const BStage& S, int n, int low,
@@ -121,7 +166,8 @@ __device__ __forceinline__ TileArgs stage_tile(const BStage& S, int n, int low,
 template <typename V, int NV, int R>
 __device__ __forceinline__ void run_stage(const BStage& S, int n, int low, bool single,
                                           const BArgs& a, V* t0, V* t1, V* psi, V* lam,
-                                          double* racc, unsigned char* plan) {
+                                          double* racc, unsigned char* plan, int rank = 0,
+                                          int team = 1) {
   const PassDev* passes;
   const POp* ops;
   const V* coefs;
@@ -135,7 +181,7 @@ __device__ __forceinline__ void run_stage(const BStage& S, int n, int low, bool 
   }
   const TileArgs ta = stage_tile<V>(S, n, low, a.runoff);
   const uint64_t ntiles = 1ull << (n - S.m);
-  for (uint64_t t = 0; t < ntiles; ++t) {
+  for (uint64_t t = rank; t < ntiles; t += team) {
     const uint64_t base = tile_base(ta, t);
     load_tile<V, NV>(psi, lam, t0, t1, ta, base, a.vec16);
     __syncthreads();
@@ -186,6 +232,7 @@ k_batch(BArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double2 red[32];
   __shared__ int job_s;
+  __shared__ unsigned slot_s;
   V* t0 = reinterpret_cast<V*>(smem_raw);
   double* racc = reinterpret_cast<double*>(smem_raw + size_t(2) * a.tile_elems * sizeof(V));
   unsigned char* plan = smem_raw + size_t(2) * a.tile_elems * sizeof(V) + kRaccBytes;
@@ -198,27 +245,56 @@ k_batch(BArgs a) {
     const BJob J = a.jobs[jb];
     const uint32_t tsize = 1u << J.m;
     V* t1 = t0 + tsize;
-    double* grads = a.results + J.grad_off;
     const bool single = (J.m == J.n);
-    V* psi = static_cast<V*>(a.work) + (size_t)blockIdx.x * a.work_stride;
+    const int team = J.team, rank = J.rank;
+    unsigned* arrive = a.team_sync + 4 * (size_t)J.team_id;
+    unsigned rounds = 0;
+    auto barrier = [&]() {
+      if (team > 1) team_barrier(arrive, (unsigned)team * ++rounds, a.error);
+    };
+    // a team works in the workspace slot of its rank-0 CTA
+    unsigned slot = blockIdx.x;
+    if (team > 1) {
+      if (rank == 0 && threadIdx.x == 0) {
+        asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(arrive + 1), "r"(blockIdx.x + 1u)
+                     : "memory");
+      }
+      barrier();
+      if (threadIdx.x == 0) {
+        unsigned v;
+        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(arrive + 1) : "memory");
+        slot_s = v ? v - 1u : blockIdx.x;
+      }
+      __syncthreads();
+      slot = slot_s;
+    }
+    V* psi = static_cast<V*>(a.work) + (size_t)slot * a.work_stride;
     V* lam = psi + ((size_t)1 << J.n);
     const uint64_t N = 1ull << J.n;
-    // (gradient accumulators were zeroed with the results before the launch)
+    // gradients: straight into the results for one CTA, else into this
+    // member's row of the team's partial sums (summed in rank order at the end)
+    double* grads = team > 1 ? a.team_part + J.part_off + team + (size_t)rank * J.nparams
+                             : a.results + J.grad_off;
+    // (results and partial sums were zeroed before the launch)
 
     // ---- psi = |0...0> ----
     if (single) {
       for (uint32_t e = threadIdx.x; e < tsize; e += blockDim.x)
         t0[phys<V>(e)] = from_d2<V>(make_double2(e == 0 ? 1.0 : 0.0, 0.0));
     } else {
-      for (uint64_t e = threadIdx.x; e < N; e += blockDim.x)
+      for (uint64_t e = (uint64_t)rank * blockDim.x + threadIdx.x; e < N;
+           e += (uint64_t)team * blockDim.x)
         psi[e] = from_d2<V>(make_double2(e == 0 ? 1.0 : 0.0, 0.0));
     }
     __syncthreads();
+    barrier();
 
     // ---- forward ----
-    for (int s = 0; s < J.nfwd; ++s)
+    for (int s = 0; s < J.nfwd; ++s) {
       run_stage<V, 1, RF>(a.stages[J.fwd0 + s], J.n, J.low, single, a, t0, t1, psi, lam, racc,
-                          plan);
+                          plan, rank, team);
+      barrier();
+    }
 
     // ---- lambda = H psi, E = <psi|H|psi> ----
     double e = 0.0;
@@ -226,9 +302,12 @@ k_batch(BArgs a) {
       if (single) {
         for (uint32_t el = threadIdx.x; el < tsize; el += blockDim.x) t1[el] = from_d2<V>(make_double2(0.0, 0.0));
       } else {
-        for (uint64_t el = threadIdx.x; el < N; el += blockDim.x) lam[el] = from_d2<V>(make_double2(0.0, 0.0));
+        for (uint64_t el = (uint64_t)rank * blockDim.x + threadIdx.x; el < N;
+             el += (uint64_t)team * blockDim.x)
+          lam[el] = from_d2<V>(make_double2(0.0, 0.0));
       }
       __syncthreads();
+      barrier();
     }
     for (int g = 0; g < J.ngrp; ++g) {
       const BGroup G = a.groups[J.grp0 + g];
@@ -243,7 +322,7 @@ k_batch(BArgs a) {
         for (int j = 0; j < 32; ++j) ta.bits[j] = G.bits[j];
         ta.runoff = a.runoff + G.run0;
         const uint64_t ntiles = 1ull << (J.n - G.m);
-        for (uint64_t t = 0; t < ntiles; ++t) {
+        for (uint64_t t = rank; t < ntiles; t += team) {
           const uint64_t base = tile_base(ta, t);
           if (g > 0) load_tile<V, 2>(psi, lam, t0, t1, ta, base, a.vec16);
           else load_tile<V, 1>(psi, nullptr, t0, nullptr, ta, base, a.vec16);
@@ -253,17 +332,21 @@ k_batch(BArgs a) {
           store_tile<V, 1>(lam, nullptr, t1, nullptr, ta, base, a.vec16);
           __syncthreads();
         }
+        barrier();
       }
     }
     const double2 et = block_sum(make_double2(e, 0.0), red);
-    if (threadIdx.x == 0) a.results[J.circ] = et.x;
+    if (threadIdx.x == 0) {
+      if (team > 1) a.team_part[J.part_off + rank] = et.x;
+      else a.results[J.circ] = et.x;
+    }
     __syncthreads();
 
     // ---- backward: uncompute psi and lambda, gradient terms in-tile ----
     for (int s = 0; s < J.nbwd; ++s) {
       const BStage S = a.stages[J.bwd0 + s];
       for (int i = threadIdx.x; i < S.nred * kRedWarps; i += blockDim.x) racc[i] = 0.0;
-      run_stage<V, 2, RB>(S, J.n, J.low, single, a, t0, t1, psi, lam, racc, plan);
+      run_stage<V, 2, RB>(S, J.n, J.low, single, a, t0, t1, psi, lam, racc, plan, rank, team);
       // the stage's gradient terms, summed over warps in a fixed order by one
       // thread (parameters may repeat within a stage)
       if (threadIdx.x == 0) {
@@ -275,6 +358,22 @@ k_batch(BArgs a) {
         }
       }
       __syncthreads();
+      barrier();
+    }
+    // a team's energy and gradients: rank 0 sums the members' rows in rank order
+    barrier();
+    if (team > 1 && rank == 0) {
+      const double* part = a.team_part + J.part_off;
+      if (threadIdx.x == 0) {
+        double et2 = 0.0;
+        for (int r = 0; r < team; ++r) et2 += part[r];
+        a.results[J.circ] = et2;
+      }
+      for (int q = threadIdx.x; q < J.nparams; q += blockDim.x) {
+        double t = 0.0;
+        for (int r = 0; r < team; ++r) t += part[team + (size_t)r * J.nparams + q];
+        a.results[J.grad_off + q] = t;
+      }
     }
     __syncthreads();
   }
@@ -376,6 +475,11 @@ qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate*
     J.m = m;
     J.low = lo;
     J.circ = c;
+    J.team = 1;
+    J.rank = 0;
+    J.team_id = 0;
+    J.nparams = nparams[c];
+    J.part_off = 0;
     J.grad_off = (int64_t)goff;
     b->grad_off[c] = goff - ncirc;
     b->nparams[c] = nparams[c];
@@ -463,6 +567,57 @@ qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate*
   std::stable_sort(jobs.begin(), jobs.end(), [](const BJob& x, const BJob& y) {
     return ((double)(1ull << x.n) * (x.nfwd + x.nbwd + 1)) > ((double)(1ull << y.n) * (y.nfwd + y.nbwd + 1));
   });
+  // launch shape (every CTA resident: the team barriers rely on it)
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (qsv_status st = cuda_status(cudaFuncSetAttribute(k_batch<V, RF, RB>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)smem), "batch smem attribute"))
+    return st;
+  int per_sm = 0;
+  const int threads = 1 << (M - RB) < 32 ? 32 : 1 << (M - RB);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<V, RF, RB>, threads, smem);
+  if (opts && opts->ctas_per_sm > 0) per_sm = std::min(per_sm, opts->ctas_per_sm);
+  if (per_sm < 1) return fail(QSV_ERROR_NOT_SUPPORTED, "batch kernel does not fit an SM");
+  int blocks = sms * per_sm;
+  const size_t stride = (size_t(2) << nmax);  // elements per CTA slot (psi + lambda)
+  if (nmax > M) {  // every CTA needs a slot: at most 8 GiB of workspace in all
+    const size_t cap = std::max<size_t>(1, (size_t(8) << 30) / (stride * sizeof(V)));
+    blocks = (int)std::min<size_t>((size_t)blocks, cap);
+  }
+  // circuits larger than a tile become teams: one job per member, ranks
+  // consecutive, at most max_team members and about two tiles per member
+  // per stage, and never more than half the grid
+  const int max_team = (opts && opts->max_team > 0) ? opts->max_team : 16;
+  std::vector<BJob> entries;
+  size_t part = 0;
+  int nteams = 0;
+  for (const BJob& J0 : jobs) {
+    int T = 1;
+    if (J0.n > J0.m) {
+      const uint64_t ntiles = 1ull << (J0.n - J0.m);
+      T = (int)std::min<uint64_t>((uint64_t)max_team, std::max<uint64_t>(1, ntiles / 2));
+      T = std::max(1, std::min(T, blocks / 2));
+    }
+    if (T == 1) {
+      entries.push_back(J0);
+      continue;
+    }
+    for (int r = 0; r < T; ++r) {
+      BJob J = J0;
+      J.team = T;
+      J.rank = r;
+      J.team_id = nteams;
+      J.part_off = (int64_t)part;
+      entries.push_back(J);
+    }
+    part += (size_t)T * (1 + (size_t)J0.nparams);
+    ++nteams;
+  }
+  jobs.swap(entries);
+  b->njobs = (int)jobs.size();
+  b->nteams = nteams;
 
   auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
   size_t off = 0;
@@ -487,36 +642,29 @@ qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate*
   put(b->off_terms, terms.data(), terms.size() * sizeof(BTerm));
   put(b->off_red, plan.red_slots.data(), plan.red_slots.size() * sizeof(int32_t));
 
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (qsv_status st = cuda_status(cudaFuncSetAttribute(k_batch<V, RF, RB>,
-                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       (int)smem), "batch smem attribute"))
-    return st;
-  int per_sm = 0;
-  const int threads = 1 << (M - RB) < 32 ? 32 : 1 << (M - RB);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<V, RF, RB>, threads, smem);
-  if (opts && opts->ctas_per_sm > 0) per_sm = std::min(per_sm, opts->ctas_per_sm);
-  if (per_sm < 1) return fail(QSV_ERROR_NOT_SUPPORTED, "batch kernel does not fit an SM");
-  b->blocks = std::min<int>(sms * per_sm, ncirc);
+  // every CTA can hold a team member, but a grid smaller than the jobs is enough
+  b->blocks = std::min<int>(blocks, b->njobs);
   b->threads = threads;
   b->smem = smem;
   b->tile_bits = M;
-  const size_t stride = (size_t(2) << nmax);  // elements per CTA slot (psi + lambda)
-  if (nmax > M) {  // every CTA needs a slot: at most 8 GiB of workspace in all
-    const size_t cap = std::max<size_t>(1, (size_t(8) << 30) / (stride * sizeof(V)));
-    b->blocks = (int)std::min<size_t>((size_t)b->blocks, cap);
-  }
   b->work_bytes = (nmax > M) ? (size_t)b->blocks * stride * sizeof(V) : 256;
   b->nresults = goff;
   b->plan_bytes = off;
+  // results | counter | team sync words | error flag | team partial sums
+  const size_t res_bytes = (goff * sizeof(double) + 127) & ~size_t(127);
+  const size_t sync_off = res_bytes + 128;
+  const size_t err_off = sync_off + (((size_t)nteams * 4 * sizeof(unsigned) + 127) & ~size_t(127));
+  const size_t part_off = err_off + 128;
+  const size_t total = part_off + part * sizeof(double) + 128;
   if (qsv_status st = cuda_status(cudaMalloc(&b->plan, off), "batch plan")) return st;
   if (qsv_status st = cuda_status(cudaMalloc(&b->work, b->work_bytes), "batch workspace")) return st;
-  if (qsv_status st = cuda_status(cudaMalloc(&b->results, goff * sizeof(double) + 256), "batch results"))
-    return st;
-  b->counter = reinterpret_cast<unsigned*>(reinterpret_cast<unsigned char*>(b->results) +
-                                           ((goff * sizeof(double) + 127) & ~size_t(127)));
+  if (qsv_status st = cuda_status(cudaMalloc(&b->results, total), "batch results")) return st;
+  unsigned char* rb = reinterpret_cast<unsigned char*>(b->results);
+  b->counter = reinterpret_cast<unsigned*>(rb + res_bytes);
+  b->team_sync = reinterpret_cast<unsigned*>(rb + sync_off);
+  b->error = reinterpret_cast<unsigned*>(rb + err_off);
+  b->team_part = reinterpret_cast<double*>(rb + part_off);
+  b->zero_bytes = total;
   return cuda_status(cudaMemcpy(b->plan, host.data(), off, cudaMemcpyHostToDevice), "batch plan upload");
 }
 
@@ -526,7 +674,7 @@ qsv_status launch_batch(qsv_batch_s* b, cudaStream_t stream) {
   unsigned char* p = static_cast<unsigned char*>(b->plan);
   BArgs a;
   a.jobs = reinterpret_cast<const BJob*>(p + b->off_jobs);
-  a.njobs = b->ncirc;
+  a.njobs = b->njobs;
   a.stages = reinterpret_cast<const BStage*>(p + b->off_stages);
   a.passes = reinterpret_cast<const PassDev*>(p + b->off_passes);
   a.ops = reinterpret_cast<const POp*>(p + b->off_ops);
@@ -539,14 +687,15 @@ qsv_status launch_batch(qsv_batch_s* b, cudaStream_t stream) {
   a.work_stride = b->work_bytes > 256 ? b->work_bytes / sizeof(V) / b->blocks : 0;
   a.results = b->results;
   a.counter = b->counter;
+  a.team_sync = b->team_sync;
+  a.team_part = b->team_part;
+  a.error = b->error;
   a.vec16 = 1;
   a.tile_elems = 1 << b->tile_bits;
-  // zero the results (gradients accumulate) and the work counter
-  if (qsv_status st = cuda_status(cudaMemsetAsync(b->results, 0, b->nresults * sizeof(double), stream),
+  // zero the results (gradients accumulate), the work counter, the team
+  // barriers and partial sums (one memset: they share one allocation)
+  if (qsv_status st = cuda_status(cudaMemsetAsync(b->results, 0, b->zero_bytes, stream),
                                   "batch results reset"))
-    return st;
-  if (qsv_status st = cuda_status(cudaMemsetAsync(b->counter, 0, sizeof(unsigned), stream),
-                                  "batch counter reset"))
     return st;
   k_batch<V, RF, RB><<<b->blocks, b->threads, b->smem, stream>>>(a);
   count_launch();
@@ -644,8 +793,16 @@ qsv_status qsv_batch_results(qsv_batch b, void* cuda_stream, double* energies, d
                                                   b->nresults * sizeof(double),
                                                   cudaMemcpyDeviceToHost, stream), "batch results copy"))
     return st;
+  unsigned err = 0;
+  if (qsv_status st = cuda_status(cudaMemcpyAsync(&err, b->error, sizeof(err),
+                                                  cudaMemcpyDeviceToHost, stream),
+                                  "batch error flag copy"))
+    return st;
   if (qsv_status st = cuda_status(cudaStreamSynchronize(stream), "batch results synchronize"))
     return st;
+  if (err)
+    return fail(QSV_ERROR_TIMEOUT, "a team of the batch gave up waiting at a barrier "
+                                   "(results invalid)");
   if (energies) std::memcpy(energies, host.data(), b->ncirc * sizeof(double));
   if (grads && b->nresults > (size_t)b->ncirc)
     std::memcpy(grads, host.data() + b->ncirc, (b->nresults - b->ncirc) * sizeof(double));
