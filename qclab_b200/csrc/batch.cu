@@ -120,9 +120,10 @@ struct BArgs {
 };
 
 // Spins of a team barrier before it gives up (with __nanosleep(100) each,
-// tens of seconds): the persistent grid is resident and teams are handed
-// out in order, so every member arrives; the limit only bounds a broken run.
-constexpr unsigned kTeamSpinLimit = 1u << 28;
+// a few seconds): the persistent grid is resident and teams are handed out
+// in order, so every member arrives; the limit only bounds a broken run.
+// Once one barrier has given up (the error flag), the others stop waiting.
+constexpr unsigned kTeamSpinLimit = 1u << 25;
 
 // Team barrier: all T members arrive, then each waits for the k-th round
 // (arrivals >= T (k + 1)).  Global writes before it are visible after it.
@@ -139,6 +140,11 @@ __device__ __forceinline__ void team_barrier(unsigned* arrive, unsigned target, 
       if (++spins > kTeamSpinLimit) {
         atomicOr(error, 1u);
         break;
+      }
+      if ((spins & 1023u) == 0) {
+        unsigned e;
+        asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(e) : "l"(error) : "memory");
+        if (e) break;
       }
       __nanosleep(100);
     }
