@@ -237,9 +237,25 @@ __device__ __forceinline__ void op_scale(V (&x)[N], const V* __restrict__ c) {
   for (int j = 0; j < N; ++j) ip_cmulv(x[j], z);
 }
 
-// One op word: code | coefficient index << kCodeBits (gate_plan.hpp).
+// Dispatch of an op word: a two-level switch (kind, then register
+// position; device_word in gate_plan.hpp), or one switch over the dense
+// codes (op word = code | coefficient index << kCodeBits).
+#ifndef QSV_GX_NESTED
+#define QSV_GX_NESTED 1
+#endif
 template <typename V, int R>
 __device__ __forceinline__ void apply_word(V (&x)[1 << R], uint32_t w, const V* __restrict__ cf) {
+#if QSV_GX_NESTED
+  const V* __restrict__ c = cf + (w >> kWordCoefShift);
+  const uint32_t kind = w & ((1u << kKindBits) - 1u);
+  const uint32_t sub = (w >> kKindBits) & ((1u << kSubBits) - 1u);
+  if constexpr (R == 4) {
+    QSV_GX_NESTED_4
+  } else {
+    static_assert(R == 5, "register passes of 4 or 5 bits");
+    QSV_GX_NESTED_5
+  }
+#else
   const V* __restrict__ c = cf + (w >> kCodeBits);
   const uint32_t code = w & ((1u << kCodeBits) - 1u);
   if constexpr (R == 4) {
@@ -254,6 +270,7 @@ __device__ __forceinline__ void apply_word(V (&x)[1 << R], uint32_t w, const V* 
       default: __builtin_unreachable();
     }
   }
+#endif
 }
 
 // ---- the stage kernel --------------------------------------------------------
@@ -444,7 +461,11 @@ qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool 
   const size_t total = run_off + runoff.size() * sizeof(uint64_t);
   std::vector<unsigned char> host(total);
   std::memcpy(host.data(), dpass.data(), pass_bytes);
-  std::memcpy(host.data() + op_off, plan.ops.data(), plan.ops.size() * sizeof(uint32_t));
+  uint32_t* hw = reinterpret_cast<uint32_t*>(host.data() + op_off);
+  for (size_t i = 0; i < plan.ops.size(); ++i) {
+    const uint32_t w = plan.ops[i];
+    hw[i] = QSV_GX_NESTED ? device_word((int)(w & ((1u << kCodeBits) - 1u)), R, w >> kCodeBits) : w;
+  }
   V* hc = reinterpret_cast<V*>(host.data() + coef_off);
   for (size_t i = 0; i < plan.coefs.size(); ++i) hc[i] = to_elem<V>(plan.coefs[i]);
   std::memcpy(host.data() + run_off, runoff.data(), runoff.size() * sizeof(uint64_t));

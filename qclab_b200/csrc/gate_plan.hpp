@@ -67,6 +67,31 @@ static_assert(code_scale(5) < (1 << kCodeBits), "op codes exceed the code field"
 
 constexpr int kMaxR = 5;
 
+// The device op word of the two-level dispatch: kind index (bits 0-4: the
+// one-qubit kinds, then the controlled kinds, the two-qubit kinds and the
+// scale), position index within the kind (bits 5-10) and coefficient index
+// (bits 11-31).
+constexpr int kKindBits = 5, kSubBits = 6, kWordCoefShift = kKindBits + kSubBits;
+inline uint32_t device_word(int code, int R, uint32_t coef) {
+  int kind, sub;
+  if (code < base2(R)) {
+    kind = code / R;
+    sub = code % R;
+  } else if (code < base4(R)) {
+    const int r = code - base2(R);
+    kind = G_N1 + (r >> 1) / (R * R);
+    sub = r % (2 * R * R);
+  } else if (code < code_scale(R)) {
+    const int r = code - base4(R);
+    kind = G_N1 + G_N2 + r / (R * R);
+    sub = r % (R * R);
+  } else {
+    kind = G_N1 + G_N2 + G_N4;
+    sub = 0;
+  }
+  return (uint32_t)kind | ((uint32_t)sub << kKindBits) | (coef << kWordCoefShift);
+}
+
 // A register pass: R tile bits (local positions, ascending) and its ops
 // (op words, stage-relative).
 struct GxPass {

@@ -47,12 +47,51 @@ def cases(R: int) -> list[str]:
     return out
 
 
+def nested(R: int) -> list[str]:
+    """The same cases as a two-level switch: on the op kind (code / block
+    size), then on the register position(s) within the kind's block, so an
+    op costs two short compare trees instead of one over every code."""
+    out = ["switch (kind) {"]
+    n1, n2 = len(KIND1), len(KIND2)
+    for k, name in enumerate(KIND1):
+        out.append(f"case {k}: switch (sub) {{")
+        for p in range(R):
+            out.append(f"  case {p}: op1<{name}, {p}>(x, c); break;")
+        out.append("  default: __builtin_unreachable(); } break;")
+    for k, name in enumerate(KIND2):
+        out.append(f"case {n1 + k}: switch (sub) {{")
+        for t in range(R):
+            for c in range(R):
+                if t == c:
+                    continue
+                for cv in range(2):
+                    out.append(f"  case {(t * R + c) * 2 + cv}: op2<{name}, {t}, {c}, {cv}>(x, c); "
+                               f"break;")
+        out.append("  default: __builtin_unreachable(); } break;")
+    for k, name in enumerate(KIND4):
+        out.append(f"case {n1 + n2 + k}: switch (sub) {{")
+        for p0 in range(R):
+            for p1 in range(p0):
+                out.append(f"  case {p0 * R + p1}: op4<{name}, {p0}, {p1}>(x, c); break;")
+        out.append("  default: __builtin_unreachable(); } break;")
+    out.append(f"case {n1 + n2 + len(KIND4)}: op_scale(x, c); break;")
+    out.append("default: __builtin_unreachable();")
+    out.append("}")
+    return out
+
+
 def main() -> None:
     lines = ["// Generated by gen_gate_cases.py -- do not edit.",
              "// Switch cases of apply_word (apply_gates.cu) for R = 4 and R = 5 register bits."]
     for R in (4, 5):
         lines.append(f"#define QSV_GX_CASES_{R} \\")
         body = cases(R)
+        for i, c in enumerate(body):
+            lines.append("  " + c + (" \\" if i + 1 < len(body) else ""))
+        lines.append("")
+    for R in (4, 5):
+        lines.append(f"#define QSV_GX_NESTED_{R} \\")
+        body = nested(R)
         for i, c in enumerate(body):
             lines.append("  " + c + (" \\" if i + 1 < len(body) else ""))
         lines.append("")
