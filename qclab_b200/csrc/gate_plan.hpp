@@ -51,6 +51,11 @@ enum Kind2 : int { G_CX, G_CGEN2, G_CNEG, G_CPH, G_N2 };
 // two-qubit kinds on positions p0 > p1, slots (j, j|p0, j|p1, j|p0|p1):
 // SWAP/ISWAP exchange slots 1 and 2 (ISWAP times z), GEN4 a 4x4 (row-major)
 enum Kind4 : int { G_SWAP, G_ISWAP, G_GEN4, G_N4 };
+// gradient terms of the two-vector (adjoint) sweeps at register position p:
+// Im <lam| X_p |psi>, Re <lam| Y_p |psi> (= Im(i <lam|Y_p|psi>)) and
+// Im <lam| Z_p |psi>, the derivatives of RotationX/Y/Z (lower.hpp:
+// generator_of, weight 1, no projector)
+enum KindR : int { G_RDX, G_RDY, G_RDZ, G_NR };
 
 // Dense case codes for R register bits (holes where p = q are never used).
 constexpr int code1(int R, int k, int p) { return k * R + p; }
@@ -62,8 +67,10 @@ constexpr int base4(int R) { return base2(R) + G_N2 * R * R * 2; }
 constexpr int code4(int R, int k, int p0, int p1) { return base4(R) + (k * R + p0) * R + p1; }
 // x *= z for every register (the stage's kappa)
 constexpr int code_scale(int R) { return base4(R) + G_N4 * R * R; }
+constexpr int code_red(int R, int k, int p) { return code_scale(R) + 1 + k * R + p; }
 constexpr int kCodeBits = 10;  // op word = code | coefficient index << kCodeBits
-static_assert(code_scale(5) < (1 << kCodeBits), "op codes exceed the code field");
+static_assert(code_red(5, G_NR, 0) < (1 << kCodeBits), "op codes exceed the code field");
+constexpr int kMaxStageRed = 64;  // gradient terms per stage (shared-memory accumulators)
 
 constexpr int kMaxR = 5;
 
@@ -85,9 +92,13 @@ inline uint32_t device_word(int code, int R, uint32_t coef) {
     const int r = code - base4(R);
     kind = G_N1 + G_N2 + r / (R * R);
     sub = r % (R * R);
-  } else {
+  } else if (code == code_scale(R)) {
     kind = G_N1 + G_N2 + G_N4;
     sub = 0;
+  } else {
+    const int r = code - code_red(R, 0, 0);
+    kind = G_N1 + G_N2 + G_N4 + 1 + r / R;
+    sub = r % R;
   }
   return (uint32_t)kind | ((uint32_t)sub << kKindBits) | (coef << kWordCoefShift);
 }
@@ -104,6 +115,8 @@ struct GxStage {
   int m;
   int bits[64];
   size_t pass0, npasses, op0, nops, coef0, ncoef;
+  size_t red0;  // gradient terms: red_slots[red0 .. red0 + nred)
+  int nred;
 };
 
 struct GxPlan {
@@ -111,6 +124,7 @@ struct GxPlan {
   std::vector<GxPass> passes;
   std::vector<uint32_t> ops;    // code | stage-relative coefficient index << kCodeBits
   std::vector<cplx> coefs;      // FP64; converted to the element type on upload
+  std::vector<int32_t> red_slots;  // output row of each gradient term, by stage
   std::vector<GxStage> stages;
 };
 
@@ -330,6 +344,29 @@ inline void host_apply_op(cplx* x, int R, uint32_t word, const cplx* c) {
   for (int j = 0; j < N; ++j) x[j] *= c[0];  // scale
 }
 
+// Two-vector mirror: a gradient term adds its value, times c[0].real(), to
+// red[c[0].imag()]; every other op acts on both psi (x) and lambda (y).
+// (c[0].real() = |kappa|^2 of the scalars factored out of the stage's
+// earlier ops, which psi and lambda both still lack at that point.)
+inline void host_apply_op2(cplx* x, cplx* y, int R, uint32_t word, const cplx* c, double* red) {
+  const int code = (int)(word & ((1u << kCodeBits) - 1u));
+  if (code <= code_scale(R)) {
+    host_apply_op(x, R, word, c);
+    host_apply_op(y, R, word, c);
+    return;
+  }
+  const int r = code - code_red(R, 0, 0), k = r / R, p = r % R, mp = 1 << p;
+  cplx s(0.0, 0.0);
+  for (int j = 0; j < (1 << R); ++j) {
+    const int f = (k == G_RDZ) ? j : (j ^ mp);
+    double sg = 1.0;
+    if (k == G_RDY) sg = ((f >> p) & 1) ? -1.0 : 1.0;
+    if (k == G_RDZ) sg = ((j >> p) & 1) ? -1.0 : 1.0;
+    s += std::conj(y[j]) * sg * x[f];
+  }
+  red[(int)c[0].imag()] += c[0].real() * ((k == G_RDY) ? s.real() : s.imag());
+}
+
 // ---- lane order ----------------------------------------------------------------
 // The tile bits that a pass's register-group index g spreads over (all
 // tile bits outside the pass), lowest g bit first, chosen so that the lanes
@@ -374,16 +411,29 @@ inline int lane_order(const int* pos, int R, int m, size_t elem_bytes, int* orde
 // Plans `gates` (single-vector items) for an n-qubit state with tiles of 2^m
 // amplitudes (`low` contiguous low bits) and register passes of R bits.
 // Returns false if an item cannot run on this engine.
+// With two_vector, gradient terms (SH_RED items of the adjoint's backward
+// list) become RDX/RDY/RDZ ops, at most kMaxStageRed per stage.
 inline bool pack_gate_plan(const std::vector<Lowered>& gates, int n, int m, int low, int R,
-                           int max_gates, size_t plan_cap, size_t elem_bytes, GxPlan* out) {
+                           int max_gates, size_t plan_cap, size_t elem_bytes, GxPlan* out,
+                           bool two_vector = false) {
   out->R = R;
   // every tile needs a bit outside its contiguous low bits unless it holds
   // the whole state
   if (m < R || R > kMaxR || (low >= m && m < n)) return false;
-  for (const Lowered& L : gates)
-    if (L.shape == SH_RED) return false;
+  for (const Lowered& L : gates) {
+    if (L.shape != SH_RED) continue;
+    if (!two_vector) return false;
+    // the generators this engine evaluates: one X, Y or Z factor, weight 1
+    const Generator& g = L.gen;
+    const uint64_t b = g.f | g.zy;
+    if (g.pm || g.w != 1 || __builtin_popcountll(b) != 1) return false;
+    const bool x = g.f == b && g.zy == 0 && g.ny == 0, y = g.f == b && g.zy == b && g.ny == 1,
+               z = g.f == 0 && g.zy == b && g.ny == 0;
+    if (!(x || y || z)) return false;
+  }
   const std::vector<Stage> stages =
-      plan_stages(gates, n, m, low, max_gates, 0, plan_cap, elem_bytes);
+      plan_stages(gates, n, m, low, max_gates, two_vector ? kMaxStageRed : 0, plan_cap,
+                  elem_bytes);
   std::vector<GxOp> ops;
   for (const Stage& stg : stages) {
     GxStage gs;
@@ -392,6 +442,8 @@ inline bool pack_gate_plan(const std::vector<Lowered>& gates, int n, int m, int 
     gs.pass0 = out->passes.size();
     gs.op0 = out->ops.size();
     gs.coef0 = out->coefs.size();
+    gs.red0 = out->red_slots.size();
+    gs.nred = 0;
     int local_of[64];
     for (int j = 0; j < 64; ++j) local_of[j] = -1;
     for (int j = 0; j < stg.m; ++j) local_of[stg.bits[j]] = j;
@@ -415,6 +467,20 @@ inline bool pack_gate_plan(const std::vector<Lowered>& gates, int n, int m, int 
       ops.clear();
       for (int oi : p.ops) {
         const Lowered& L = gates[stg.gates[oi]];
+        if (L.shape == SH_RED) {
+          // coefficient: (|kappa|^2 so far, term index)
+          const uint64_t b = L.gen.f | L.gen.zy;
+          const int r0 = reg_of[local_of[__builtin_ctzll(b)]];
+          const int k = L.gen.zy == 0 ? G_RDX : (L.gen.f == 0 ? G_RDZ : G_RDY);
+          if (gs.nred >= kMaxStageRed) return false;
+          GxOp op;
+          op.code = code_red(R, k, r0);
+          op.ncoef = 1;
+          op.c[0] = cplx(std::norm(kappa), (double)gs.nred++);
+          ops.push_back(op);
+          out->red_slots.push_back(L.slot);
+          continue;
+        }
         const bool one = L.shape == SH_PAIR || L.shape == SH_HALF;
         const int r0 = reg_of[local_of[L.t0]];
         const int r1 = one ? 0 : reg_of[local_of[L.t1]];
@@ -429,11 +495,12 @@ inline bool pack_gate_plan(const std::vector<Lowered>& gates, int n, int m, int 
       }
       gp.op0 = (int32_t)(out->ops.size() - gs.op0);
       gp.nops = (int32_t)ops.size();
-      for (const GxOp& o : ops) {
+      for (size_t i = 0; i < ops.size(); ++i) {
+        const GxOp& o = ops[i];
         const size_t ci = out->coefs.size() - gs.coef0;
         if (ci >= (size_t(1) << (32 - kCodeBits))) return false;
         out->ops.push_back((uint32_t)o.code | ((uint32_t)ci << kCodeBits));
-        for (int i = 0; i < o.ncoef; ++i) out->coefs.push_back(o.c[i]);
+        for (int c = 0; c < o.ncoef; ++c) out->coefs.push_back(o.c[c]);
       }
       out->passes.push_back(gp);
     }
@@ -446,8 +513,11 @@ inline bool pack_gate_plan(const std::vector<Lowered>& gates, int n, int m, int 
 }
 
 // Host mirror of a whole plan on an n-qubit state (tests): stage by stage,
-// tile by tile, pass by pass, exactly the order of the device kernel.
-inline void host_apply_plan(const GxPlan& P, int n, std::vector<cplx>& v) {
+// tile by tile, pass by pass, exactly the order of the device kernel.  With
+// lam (a second vector), every op acts on both and gradient terms add into
+// rows[red_slots[...]].
+inline void host_apply_plan(const GxPlan& P, int n, std::vector<cplx>& v,
+                            std::vector<cplx>* lam = nullptr, double* rows = nullptr) {
   const int R = P.R;
   for (const GxStage& s : P.stages) {
     uint64_t S = 0;
@@ -456,7 +526,8 @@ inline void host_apply_plan(const GxPlan& P, int n, std::vector<cplx>& v) {
     for (int b = 0; b < n; ++b)
       if (!((S >> b) & 1ull)) outside.push_back(b);
     const uint64_t ntiles = 1ull << (n - s.m);
-    std::vector<cplx> tile(size_t(1) << s.m);
+    std::vector<cplx> tile(size_t(1) << s.m), tile2(lam ? tile.size() : 0);
+    std::vector<double> red(s.nred > 0 ? s.nred : 1, 0.0);
     for (uint64_t t = 0; t < ntiles; ++t) {
       uint64_t base = 0;
       for (size_t k = 0; k < outside.size(); ++k)
@@ -468,6 +539,8 @@ inline void host_apply_plan(const GxPlan& P, int n, std::vector<cplx>& v) {
         return g;
       };
       for (uint32_t e = 0; e < tile.size(); ++e) tile[e] = v[global(e)];
+      if (lam)
+        for (uint32_t e = 0; e < tile.size(); ++e) tile2[e] = (*lam)[global(e)];
       for (size_t pi = s.pass0; pi < s.pass0 + s.npasses; ++pi) {
         const GxPass& gp = P.passes[pi];
         uint32_t pm = 0;
@@ -475,7 +548,7 @@ inline void host_apply_plan(const GxPlan& P, int n, std::vector<cplx>& v) {
         std::vector<int> rest;
         for (int j = 0; j < s.m; ++j)
           if (!((pm >> j) & 1u)) rest.push_back(j);
-        cplx x[1 << kMaxR];
+        cplx x[1 << kMaxR], y[1 << kMaxR];
         for (uint32_t g = 0; g < (1u << (s.m - R)); ++g) {
           uint32_t tb = 0;
           for (size_t k = 0; k < rest.size(); ++k)
@@ -487,15 +560,26 @@ inline void host_apply_plan(const GxPlan& P, int n, std::vector<cplx>& v) {
             return e;
           };
           for (int j = 0; j < (1 << R); ++j) x[j] = tile[reg(j)];
+          if (lam)
+            for (int j = 0; j < (1 << R); ++j) y[j] = tile2[reg(j)];
           for (int o = 0; o < gp.nops; ++o) {
             const uint32_t w = P.ops[s.op0 + gp.op0 + o];
-            host_apply_op(x, R, w, P.coefs.data() + s.coef0 + (w >> kCodeBits));
+            if (lam)
+              host_apply_op2(x, y, R, w, P.coefs.data() + s.coef0 + (w >> kCodeBits), red.data());
+            else
+              host_apply_op(x, R, w, P.coefs.data() + s.coef0 + (w >> kCodeBits));
           }
           for (int j = 0; j < (1 << R); ++j) tile[reg(j)] = x[j];
+          if (lam)
+            for (int j = 0; j < (1 << R); ++j) tile2[reg(j)] = y[j];
         }
       }
       for (uint32_t e = 0; e < tile.size(); ++e) v[global(e)] = tile[e];
+      if (lam)
+        for (uint32_t e = 0; e < tile.size(); ++e) (*lam)[global(e)] = tile2[e];
     }
+    if (rows)
+      for (int r = 0; r < s.nred; ++r) rows[P.red_slots[s.red0 + r]] += red[r];
   }
 }
 

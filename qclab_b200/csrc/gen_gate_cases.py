@@ -1,6 +1,6 @@
 """Writes gate_cases.inc: the switch cases of the gate-specialised stage
 kernel (apply_gates.cu), one per op kind and register position(s), for
-register passes of R = 4 and R = 5 bits.
+register passes of R = 3, 4 and 5 bits.
 
 Every case label carries a static_assert against the host's code formula
 (gate_plan.hpp: code1 / code2 / code4 / code_scale), so the two cannot drift
@@ -83,13 +83,13 @@ def nested(R: int) -> list[str]:
 def main() -> None:
     lines = ["// Generated by gen_gate_cases.py -- do not edit.",
              "// Switch cases of apply_word (apply_gates.cu) for R = 4 and R = 5 register bits."]
-    for R in (4, 5):
+    for R in (3, 4, 5):
         lines.append(f"#define QSV_GX_CASES_{R} \\")
         body = cases(R)
         for i, c in enumerate(body):
             lines.append("  " + c + (" \\" if i + 1 < len(body) else ""))
         lines.append("")
-    for R in (4, 5):
+    for R in (3, 4, 5):
         lines.append(f"#define QSV_GX_NESTED_{R} \\")
         body = nested(R)
         for i, c in enumerate(body):

@@ -76,3 +76,54 @@ def test_brick_circuit(binary, tmp_path, R):
     assert np.max(np.abs(got - want)) < 1e-12
     # every gate is one op, plus one scale op per stage
     assert ops <= len(recs) + stages
+
+
+@pytest.mark.parametrize("R,m,low", [(3, 8, 2), (4, 9, 3), (4, 11, 2)])
+def test_adjoint_gradient_terms(binary, tmp_path, R, m, low):
+    """The backward list of qsv_adjoint_gradient on two vectors (gradient
+    terms as RDX/RDY/RDZ ops) against parameter shift on the oracle."""
+    from qclab_b200 import gates as G
+    from qclab_b200.circuit import QCircuit
+    from qclab_b200.observable import ising
+    n = 10
+    rng = np.random.default_rng(R * 10 + m)
+    c = QCircuit(n)
+    for layer in range(3):
+        for q in range(n):
+            kind = (G.RotationX, G.RotationY, G.RotationZ)[int(rng.integers(0, 3))]
+            c.push_back(kind(q, float(rng.uniform(0, 6.28))))
+        for q in range(layer % 2, n - 1, 2):
+            c.push_back(G.CNOT(q, q + 1) if rng.random() < 0.5 else G.CZ(q, q + 1))
+        c.push_back(G.Hadamard(int(rng.integers(0, n))))
+    recs = c.gate_records(np.complex128, number_params=True)
+    terms = ising(n).matrix_free_terms()
+    psi = np.zeros(1 << n, dtype=np.complex128)
+    psi[0] = 1
+    oracle.apply(psi, recs)
+    lam = oracle.observable_apply(psi, terms)
+    rp, pp, lp, op_ = (tmp_path / f for f in ("r.bin", "p.bin", "l.bin", "o.bin"))
+    rp.write_bytes(recs.tobytes())
+    pp.write_bytes(psi.tobytes())
+    lp.write_bytes(lam.tobytes())
+    r = subprocess.run([str(binary), "adjoint", str(n), str(R), str(m), str(low), str(rp), str(pp),
+                        str(lp), str(op_)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    rows = np.frombuffer(op_.read_bytes(), dtype=np.float64)
+    params = [int(recs[k]["param"]) for k in range(len(recs) - 1, -1, -1) if recs[k]["param"] >= 0]
+    grad = np.zeros(int(recs["param"].max()) + 1)
+    for slot, p in enumerate(params):
+        grad[p] += rows[slot]
+
+    def energy(rr):
+        x = np.zeros(1 << n, dtype=np.complex128)
+        x[0] = 1
+        oracle.apply(x, rr)
+        return oracle.expectation(x, terms)
+
+    from qclab_b200.gradients import _shifted
+    for k in range(len(recs)):
+        p = int(recs[k]["param"])
+        if p < 0:
+            continue
+        ps = 0.5 * (energy(_shifted(recs, k, np.pi / 2)) - energy(_shifted(recs, k, -np.pi / 2)))
+        assert abs(grad[p] - ps) < 1e-10, (p, grad[p], ps)
