@@ -1234,6 +1234,13 @@ qsv_status execute_typed(const ExecArgs& x) {
         if (st != QSV_ERROR_NOT_SUPPORTED) return st;
       }
     }
+    // two-vector (adjoint) sweeps: the gate engine unless the sparse passes
+    // are asked for (engine 1), with the tiles the caller sized its partial
+    // sums for (fused_tiles)
+    if (x.nv == 2 && (!opts || opts->engine != 1)) {
+      const qsv_status st = execute_gates<V>(x, m, low, max_gates, vec16);
+      if (st != QSV_ERROR_NOT_SUPPORTED) return st;
+    }
   }
   if (x.nv == 1 && x.nslots == 0) {
     const int md = dmma_tile_bits<V>(n, opts);
@@ -1327,15 +1334,17 @@ qsv_status execute_typed(const ExecArgs& x) {
     for (auto& e : ev) cudaEventDestroy(e);
     if (st) return st;
   }
-  if (x.nslots > 0) {
-    k_rows<<<x.nslots, 256, 0, s->stream>>>(x.partial, (int)ntiles, x.rows_out);
-    count_launch();
-    if (qsv_status st = cuda_status(cudaGetLastError(), "row reduction launch")) return st;
-  }
+  if (x.nslots > 0) return reduce_rows(x, ntiles);
   return QSV_SUCCESS;
 }
 
 }  // namespace
+
+qsv_status reduce_rows(const ExecArgs& x, uint64_t ntiles) {
+  k_rows<<<x.nslots, 256, 0, x.s->stream>>>(x.partial, (int)ntiles, x.rows_out);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "row reduction launch");
+}
 
 int default_tile_bits(size_t eb, int nv) { return (eb >= 16 ? 12 : 13) - (nv == 2 ? 1 : 0); }
 

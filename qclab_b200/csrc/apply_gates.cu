@@ -237,40 +237,66 @@ __device__ __forceinline__ void op_scale(V (&x)[N], const V* __restrict__ c) {
   for (int j = 0; j < N; ++j) ip_cmulv(x[j], z);
 }
 
-// Dispatch of an op word: a two-level switch (kind, then register
-// position; device_word in gate_plan.hpp), or one switch over the dense
-// codes (op word = code | coefficient index << kCodeBits).
-#ifndef QSV_GX_NESTED
-#define QSV_GX_NESTED 1
-#endif
-template <typename V, int R>
-__device__ __forceinline__ void apply_word(V (&x)[1 << R], uint32_t w, const V* __restrict__ cf) {
-#if QSV_GX_NESTED
+// A gradient term of a two-vector sweep: c[0] = (|kappa|^2 pending in the
+// stage, term index); the thread's sum over its registers of
+//   RDX: conj(lam_j) psi_{j^p}             -> Im
+//   RDY: conj(lam_j) (-1)^{bit p of j^p} psi_{j^p} -> Re  (= Im(i s))
+//   RDZ: conj(lam_j) (-1)^{bit p of j} psi_j      -> Im
+// in FP64, reduced over the warp into the term's shared-memory accumulator
+// (stage_exec.cuh: red_accumulate).
+template <int K, int P, typename V, int N>
+__device__ __forceinline__ void red_op(const V (&x)[N], const V (&y)[N], const V* __restrict__ c,
+                                       double* racc, unsigned lanes) {
+  constexpr int M = 1 << P;
+  double sr = 0.0, si = 0.0;
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    const int f = (K == G_RDZ) ? j : (j ^ M);
+    const bool neg = (K == G_RDY) ? ((f & M) != 0) : (K == G_RDZ) ? ((j & M) != 0) : false;
+    const double2 a = to_d2(y[j]), b = to_d2(x[f]);
+    const double re = fma(a.x, b.x, a.y * b.y), im = fma(a.x, b.y, -a.y * b.x);
+    if (neg) {
+      sr -= re;
+      si -= im;
+    } else {
+      sr += re;
+      si += im;
+    }
+  }
+  const double2 cc = to_d2(c[0]);
+  fx::red_accumulate(cc.x * ((K == G_RDY) ? sr : si), (int)cc.y, racc, lanes);
+}
+
+// One op word (device_word in gate_plan.hpp): kind (bits 0-4), register
+// position index (bits 5-10), coefficient index (bits 11-31); a two-level
+// switch (gate_cases.inc).  With NV = 2 every op acts on psi (x) and
+// lambda (y) and gradient terms accumulate into racc.
+template <typename V, int R, int NV>
+__device__ __forceinline__ void apply_word(V (&x)[1 << R], V (&y)[1 << R], uint32_t w,
+                                           const V* __restrict__ cf, double* racc,
+                                           unsigned lanes) {
   const V* __restrict__ c = cf + (w >> kWordCoefShift);
   const uint32_t kind = w & ((1u << kKindBits) - 1u);
   const uint32_t sub = (w >> kKindBits) & ((1u << kSubBits) - 1u);
-  if constexpr (R == 4) {
+#define GX1(f)                      \
+  do {                              \
+    f(x, c);                        \
+    if constexpr (NV == 2) f(y, c); \
+  } while (0)
+#define GXR(K, P)                                                   \
+  do {                                                              \
+    if constexpr (NV == 2) red_op<K, P>(x, y, c, racc, lanes);      \
+  } while (0)
+  if constexpr (R == 3) {
+    QSV_GX_NESTED_3
+  } else if constexpr (R == 4) {
     QSV_GX_NESTED_4
   } else {
-    static_assert(R == 5, "register passes of 4 or 5 bits");
+    static_assert(R == 5, "register passes of 3, 4 or 5 bits");
     QSV_GX_NESTED_5
   }
-#else
-  const V* __restrict__ c = cf + (w >> kCodeBits);
-  const uint32_t code = w & ((1u << kCodeBits) - 1u);
-  if constexpr (R == 4) {
-    switch (code) {
-      QSV_GX_CASES_4
-      default: __builtin_unreachable();
-    }
-  } else {
-    static_assert(R == 5, "register passes of 4 or 5 bits");
-    switch (code) {
-      QSV_GX_CASES_5
-      default: __builtin_unreachable();
-    }
-  }
-#endif
+#undef GX1
+#undef GXR
 }
 
 // ---- the stage kernel --------------------------------------------------------
@@ -296,6 +322,10 @@ struct GxArgs {
   const uint32_t* ops;
   const void* coefs;  // V
   int vec16;
+  // two-vector sweeps: the stage's gradient terms -> partial[slot][tile]
+  int nred;
+  const int32_t* red_slots;
+  double* partial;
 };
 
 template <int R>
@@ -307,26 +337,34 @@ __device__ __forceinline__ uint32_t reg_off(uint32_t ptb, const uint32_t (&boff)
   return o;
 }
 
-template <typename V, int R, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_gates(V* __restrict__ v0, GxArgs a) {
+template <typename V, int R, int NT, int MINB, int NV>
+__global__ void __launch_bounds__(NT, MINB) k_gates(V* __restrict__ v0, V* __restrict__ v1,
+                                                    GxArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t size = 1u << a.ta.m;
   V* t0 = reinterpret_cast<V*>(smem_raw);
-  // the stage's plan, copied once per CTA: passes | op words | coefficients
-  unsigned char* pp = smem_raw + size_t(size) * sizeof(V);
+  V* t1 = t0 + size;
+  // two-vector sweeps: the gradient terms' per-warp accumulators after the
+  // tiles; then the stage's plan, copied once per CTA: passes | op words |
+  // coefficients
+  double* racc = reinterpret_cast<double*>(smem_raw + size_t(NV) * size * sizeof(V));
+  unsigned char* pp = smem_raw + size_t(NV) * size * sizeof(V) + (NV == 2 ? fx::kRaccBytes : 0);
   unsigned char* po = pp + align16(size_t(a.npasses) * sizeof(GxPassDev));
   unsigned char* pc = po + align16(size_t(a.nops) * sizeof(uint32_t));
   copy_words(pp, a.passes, size_t(a.npasses) * sizeof(GxPassDev));
   copy_words(po, a.ops, size_t(a.nops) * sizeof(uint32_t));
   copy_words(pc, a.coefs, size_t(a.ncoef) * sizeof(V));
+  if (NV == 2)
+    for (int i = threadIdx.x; i < a.nred * fx::kRedWarps; i += blockDim.x) racc[i] = 0.0;
   const GxPassDev* passes = reinterpret_cast<const GxPassDev*>(pp);
   const uint32_t* ops = reinterpret_cast<const uint32_t*>(po);
   const V* coefs = reinterpret_cast<const V*>(pc);
   const uint64_t base = tile_base(a.ta, blockIdx.x);
-  load_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
+  load_tile<V, NV>(v0, v1, t0, t1, a.ta, base, a.vec16);
   __syncthreads();
   constexpr int N = 1 << R;
   const uint32_t ngroups = size >> R;
+  const unsigned lanes = blockDim.x < 32u ? blockDim.x : 32u;
   for (int pi = 0; pi < a.npasses; ++pi) {
     const GxPassDev& P = passes[pi];
     uint32_t boff[R];
@@ -341,51 +379,80 @@ __global__ void __launch_bounds__(NT, MINB) k_gates(V* __restrict__ v0, GxArgs a
       uint32_t ptb = 0;
       for (int k = 0; k < gbits; ++k)
         if ((g >> k) & 1u) ptb ^= P.goff[k];
-      V x[N];
+      V x[N], y[N];
       // register j sits at ptb ^ XOR_{k in j} boff[k]; recomputed for the
       // store rather than held across the ops
       if (pairs) {
 #pragma unroll
-        for (int j = 0; j < N; j += 2) ld_pair(t0 + reg_off<R>(ptb, boff, j), x[j], x[j + 1]);
+        for (int j = 0; j < N; j += 2) {
+          const uint32_t o = reg_off<R>(ptb, boff, j);
+          ld_pair(t0 + o, x[j], x[j + 1]);
+          if (NV == 2) ld_pair(t1 + o, y[j], y[j + 1]);
+        }
       } else {
 #pragma unroll
-        for (int j = 0; j < N; ++j) x[j] = t0[reg_off<R>(ptb, boff, j)];
+        for (int j = 0; j < N; ++j) {
+          const uint32_t o = reg_off<R>(ptb, boff, j);
+          x[j] = t0[o];
+          if (NV == 2) y[j] = t1[o];
+        }
       }
-      for (int o = 0; o < nops; ++o) apply_word<V, R>(x, ops[op0 + o], coefs);
+      for (int o = 0; o < nops; ++o) apply_word<V, R, NV>(x, y, ops[op0 + o], coefs, racc, lanes);
       if (pairs) {
 #pragma unroll
-        for (int j = 0; j < N; j += 2) st_pair(t0 + reg_off<R>(ptb, boff, j), x[j], x[j + 1]);
+        for (int j = 0; j < N; j += 2) {
+          const uint32_t o = reg_off<R>(ptb, boff, j);
+          st_pair(t0 + o, x[j], x[j + 1]);
+          if (NV == 2) st_pair(t1 + o, y[j], y[j + 1]);
+        }
       } else {
 #pragma unroll
-        for (int j = 0; j < N; ++j) t0[reg_off<R>(ptb, boff, j)] = x[j];
+        for (int j = 0; j < N; ++j) {
+          const uint32_t o = reg_off<R>(ptb, boff, j);
+          t0[o] = x[j];
+          if (NV == 2) t1[o] = y[j];
+        }
       }
     }
     __syncthreads();
   }
-  store_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
+  store_tile<V, NV>(v0, v1, t0, t1, a.ta, base, a.vec16);
+  if (NV == 2) {  // the last pass ended with a barrier: racc is complete
+    const int warps = fx::red_warps();
+    for (int r = threadIdx.x; r < a.nred; r += blockDim.x) {
+      double t = 0.0;
+      for (int w = 0; w < warps; ++w) t += racc[r * fx::kRedWarps + w];
+      a.partial[(size_t)a.red_slots[r] * gridDim.x + blockIdx.x] = t;
+    }
+  }
 }
 
-// Launch shapes.  A thread holds 2^R amplitudes (64 registers for
-// complex<double> with R = 4, whose op switch needs ~190 registers in all),
-// so complex<double> runs CTAs of 128 threads, two per SM by default (three
-// with qsv_fuse_opts.ctas_per_sm = 3, at 168 registers); complex<float>
-// with R = 4 runs 256-thread CTAs, three per SM (two on request), with
-// R = 5 two 128-thread CTAs.  Each thread takes ngroups / threads register
-// groups per pass.
+// Launch shapes.  A thread holds 2^R amplitudes per vector (64 registers
+// for complex<double> with R = 4, whose op switch needs ~190 registers in
+// all), so single-vector complex<double> runs CTAs of 128 threads, two per
+// SM by default (three with qsv_fuse_opts.ctas_per_sm = 3, at 168
+// registers); complex<float> with R = 4 runs 256-thread CTAs, three per SM
+// (two on request), with R = 5 two 128-thread CTAs.  Two-vector sweeps hold
+// 2 x 2^R amplitudes: R = 3 for complex<double>, 4 for complex<float>, in
+// 128-thread CTAs, two per SM.  Each thread takes ngroups / threads
+// register groups per pass.
 template <typename V> struct GxKernels;
 template <> struct GxKernels<double2> {
-  static void* get(int R, int ctas) {
+  static void* get(int R, int ctas, int nv) {
     (void)R;
-    return ctas == 3 ? (void*)k_gates<double2, 4, 128, 3> : (void*)k_gates<double2, 4, 128, 2>;
+    if (nv == 2) return (void*)k_gates<double2, 3, 128, 2, 2>;
+    return ctas == 3 ? (void*)k_gates<double2, 4, 128, 3, 1>
+                     : (void*)k_gates<double2, 4, 128, 2, 1>;
   }
-  static int threads(int R) { (void)R; return 128; }
+  static int threads(int R, int nv) { (void)R; (void)nv; return 128; }
 };
 template <> struct GxKernels<float2> {
-  static void* get(int R, int ctas) {
-    if (R == 5) return (void*)k_gates<float2, 5, 128, 2>;
-    return ctas == 2 ? (void*)k_gates<float2, 4, 256, 2> : (void*)k_gates<float2, 4, 256, 3>;
+  static void* get(int R, int ctas, int nv) {
+    if (nv == 2) return (void*)k_gates<float2, 4, 128, 2, 2>;
+    if (R == 5) return (void*)k_gates<float2, 5, 128, 2, 1>;
+    return ctas == 2 ? (void*)k_gates<float2, 4, 256, 2, 1> : (void*)k_gates<float2, 4, 256, 3, 1>;
   }
-  static int threads(int R) { return R == 5 ? 128 : 256; }
+  static int threads(int R, int nv) { return (nv == 2 || R == 5) ? 128 : 256; }
 };
 
 template <typename V> V to_elem(cplx z);
@@ -404,16 +471,19 @@ size_t gx_plan_smem(size_t npasses, size_t nops, size_t ncoef) {
 
 }  // namespace gx
 
-int gate_pass_bits(size_t elem_bytes, const qsv_fuse_opts* opts) {
-  // complex<double> passes hold 4 bits (5 would not fit the registers)
+int gate_pass_bits(size_t elem_bytes, const qsv_fuse_opts* opts, int nv) {
+  // two vectors: 3 bits (complex<double>) or 4 (complex<float>); one vector:
+  // 4 bits, or 5 for complex<float> with reg_bits = 5
+  if (nv == 2) return elem_bytes >= 16 ? 3 : 4;
   return (elem_bytes < 16 && opts && opts->reg_bits == 5) ? 5 : 4;
 }
 
 namespace {
 
 qsv_status pack_gates_for(const std::vector<Lowered>& items, int n, int m, int low, int R,
-                          int max_gates, size_t elem_bytes, gx::GxPlan* plan) {
-  if (!gx::pack_gate_plan(items, n, m, low, R, max_gates, gx::kGxPlanCap, elem_bytes, plan))
+                          int max_gates, size_t elem_bytes, gx::GxPlan* plan, int nv) {
+  if (!gx::pack_gate_plan(items, n, m, low, R, max_gates, gx::kGxPlanCap, elem_bytes, plan,
+                          nv == 2))
     return QSV_ERROR_NOT_SUPPORTED;
   return QSV_SUCCESS;
 }
@@ -425,11 +495,14 @@ qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool 
   using namespace gx;
   qsv_state_s* s = x.s;
   const int n = s->n;
-  const int R = gate_pass_bits(sizeof(V), x.opts);
+  const int nv = x.nv;
+  const int R = gate_pass_bits(sizeof(V), x.opts, nv);
   if (m < R + 1) return QSV_ERROR_NOT_SUPPORTED;
   GxPlan plan;
-  if (qsv_status st = pack_gates_for(*x.items, n, m, low, R, max_gates, sizeof(V), &plan))
+  if (qsv_status st = pack_gates_for(*x.items, n, m, low, R, max_gates, sizeof(V), &plan, nv))
     return st;
+  if (nv == 2 && x.nslots > 0 && x.partial_bytes < (size_t)x.nslots * (1ull << (n - m)) * sizeof(double))
+    return fail(QSV_ERROR_SIZE, "partial-sum buffer too small");
   if (plan.stages.empty()) return QSV_SUCCESS;
   std::vector<GxPassDev> dpass(plan.passes.size());
   std::vector<uint64_t> runoff;
@@ -458,23 +531,27 @@ qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool 
   const size_t op_off = align(pass_bytes);
   const size_t coef_off = align(op_off + plan.ops.size() * sizeof(uint32_t));
   const size_t run_off = align(coef_off + plan.coefs.size() * sizeof(V));
-  const size_t total = run_off + runoff.size() * sizeof(uint64_t);
+  const size_t red_off = align(run_off + runoff.size() * sizeof(uint64_t));
+  const size_t total = red_off + plan.red_slots.size() * sizeof(int32_t);
   std::vector<unsigned char> host(total);
   std::memcpy(host.data(), dpass.data(), pass_bytes);
   uint32_t* hw = reinterpret_cast<uint32_t*>(host.data() + op_off);
   for (size_t i = 0; i < plan.ops.size(); ++i) {
     const uint32_t w = plan.ops[i];
-    hw[i] = QSV_GX_NESTED ? device_word((int)(w & ((1u << kCodeBits) - 1u)), R, w >> kCodeBits) : w;
+    hw[i] = device_word((int)(w & ((1u << kCodeBits) - 1u)), R, w >> kCodeBits);
   }
   V* hc = reinterpret_cast<V*>(host.data() + coef_off);
   for (size_t i = 0; i < plan.coefs.size(); ++i) hc[i] = to_elem<V>(plan.coefs[i]);
   std::memcpy(host.data() + run_off, runoff.data(), runoff.size() * sizeof(uint64_t));
+  if (!plan.red_slots.empty())
+    std::memcpy(host.data() + red_off, plan.red_slots.data(),
+                plan.red_slots.size() * sizeof(int32_t));
   if (qsv_status st = ensure_scratch(s, total)) return st;
   unsigned char* dev = static_cast<unsigned char*>(s->scratch);
   if (qsv_status st = cuda_status(cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice,
                                                   s->stream), "gate plan upload"))
     return st;
-  void* kern = GxKernels<V>::get(R, x.opts ? x.opts->ctas_per_sm : 0);
+  void* kern = GxKernels<V>::get(R, x.opts ? x.opts->ctas_per_sm : 0, nv);
   if (qsv_status st = cuda_status(cudaFuncSetAttribute(kern,
                                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                        200 * 1024), "gate stage shared-memory attribute"))
@@ -482,13 +559,17 @@ qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool 
   const uint64_t ntiles = 1ull << (n - m);
   if (x.ntiles_out) *x.ntiles_out = ntiles;
   const unsigned threads =
-      (unsigned)std::min<uint64_t>((uint64_t)GxKernels<V>::threads(R), 1ull << (m - R));
+      (unsigned)std::min<uint64_t>((uint64_t)GxKernels<V>::threads(R, nv), 1ull << (m - R));
   StageTimer timer(x.opts && x.opts->profile, plan.stages.size(), s->stream);
   if (qsv_status st = timer.start()) return st;
   V* p0 = static_cast<V*>(x.v0);
+  V* p1 = static_cast<V*>(x.v1);
   for (size_t si = 0; si < plan.stages.size(); ++si) {
     const GxStage& gs = plan.stages[si];
     GxArgs a;
+    a.nred = gs.nred;
+    a.red_slots = reinterpret_cast<const int32_t*>(dev + red_off) + gs.red0;
+    a.partial = x.partial;
     a.ta.n = n;
     a.ta.m = gs.m;
     a.ta.low = low;
@@ -501,11 +582,11 @@ qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool 
     a.ops = reinterpret_cast<const uint32_t*>(dev + op_off) + gs.op0;
     a.coefs = dev + coef_off + gs.coef0 * sizeof(V);
     a.vec16 = vec16 ? 1 : 0;
-    const size_t smem =
-        (size_t(1) << gs.m) * sizeof(V) + gx_plan_smem<V>(gs.npasses, gs.nops, gs.ncoef);
+    const size_t smem = (size_t(1) << gs.m) * sizeof(V) * nv + (nv == 2 ? fx::kRaccBytes : 0) +
+                        gx_plan_smem<V>(gs.npasses, gs.nops, gs.ncoef);
     if (smem > 200 * 1024)
       return fail(QSV_ERROR_SIZE, "gate stage needs %zu bytes of shared memory", smem);
-    void* args[] = {&p0, &a};
+    void* args[] = {&p0, &p1, &a};
     if (qsv_status st = cuda_status(cudaLaunchKernel(kern, dim3((unsigned)ntiles), dim3(threads),
                                                      args, smem, s->stream),
                                     "gate stage launch"))
@@ -513,7 +594,8 @@ qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool 
     count_launch();
     if (qsv_status st = timer.mark(si)) return st;
   }
-  return timer.finish();
+  if (qsv_status st = timer.finish()) return st;
+  return nv == 2 && x.nslots > 0 ? reduce_rows(x, ntiles) : QSV_SUCCESS;
 }
 
 template qsv_status execute_gates<double2>(const ExecArgs&, int, int, int, bool);
@@ -523,8 +605,8 @@ qsv_status gate_plan_counts(const std::vector<Lowered>& items, int n, int m, int
                             const qsv_fuse_opts* opts, int max_gates, size_t elem_bytes,
                             std::vector<int>* ops, std::vector<int>* passes) {
   gx::GxPlan plan;
-  if (qsv_status st = pack_gates_for(items, n, m, low, gate_pass_bits(elem_bytes, opts),
-                                     max_gates, elem_bytes, &plan))
+  if (qsv_status st = pack_gates_for(items, n, m, low, gate_pass_bits(elem_bytes, opts, 1),
+                                     max_gates, elem_bytes, &plan, 1))
     return st;
   for (const gx::GxStage& gs : plan.stages) {
     ops->push_back((int)gs.nops);

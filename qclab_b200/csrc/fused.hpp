@@ -42,15 +42,18 @@ class StageTimer {
   std::vector<cudaEvent_t> ev_;
 };
 
-// Single-vector sweep of a complex<double> / complex<float> state on the
-// gate-specialised engine (apply_gates.cu) with tiles of 2^m amplitudes;
-// QSV_ERROR_NOT_SUPPORTED, with nothing launched, when the items do not fit
-// it.
+// Sweep of a complex<double> / complex<float> state (x.nv = 1) or of psi
+// and lambda with gradient terms (x.nv = 2) on the gate-specialised engine
+// (apply_gates.cu) with tiles of 2^m amplitudes; QSV_ERROR_NOT_SUPPORTED,
+// with nothing launched, when the items do not fit it.
 template <typename V>
 qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool vec16);
-// Register bits of its passes: 4, or 5 for 8-byte elements with
-// qsv_fuse_opts.reg_bits = 5.
-int gate_pass_bits(size_t elem_bytes, const qsv_fuse_opts* opts);
+// Register bits of its passes: single-vector 4, or 5 for 8-byte elements
+// with qsv_fuse_opts.reg_bits = 5; two-vector 3 (16-byte) or 4 (8-byte).
+int gate_pass_bits(size_t elem_bytes, const qsv_fuse_opts* opts, int nv = 1);
+// Fixed-order sum of x.partial's rows (x.nslots rows of ntiles tile sums)
+// into x.rows_out, on the state's stream.
+qsv_status reduce_rows(const ExecArgs& x, uint64_t ntiles);
 // Its plan statistics: ops and passes per stage.
 qsv_status gate_plan_counts(const std::vector<Lowered>& items, int n, int m, int low,
                             const qsv_fuse_opts* opts, int max_gates, size_t elem_bytes,
