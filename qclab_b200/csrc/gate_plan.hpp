@@ -138,13 +138,54 @@ struct GxOp {
 inline bool is_real(cplx z) { return z.imag() == 0.0; }
 inline bool is_imag(cplx z) { return z.real() == 0.0; }
 
+// Coefficients are applied in the element's precision.  In float, a
+// rounded coefficient would make a gate slightly non-unitary, and since the
+// same gate acts on every amplitude the norm error is coherent: over
+// thousands of gates it grows like a random walk (1e-6 over a 32-qubit brick
+// of depth 100).  So the packer rounds first and compensates:
+//   - a shear's scalar is derived from its rounded coefficient, which keeps
+//     kappa [[1, t], [-t, 1]] (and the RotationX forms) exactly unitary;
+//   - a phase is the float pair nearest to it with |z| closest to |z_exact|;
+//   - the stage scale kappa carries its rounding error into the next stage.
+inline double round_to(double x, bool f32) { return f32 ? (double)(float)x : x; }
+
+// The float pair near z (a few ulps each way) whose modulus is closest to |z|.
+inline cplx unit_round(cplx z, bool f32) {
+  if (!f32) return z;
+  const double target = std::abs(z);
+  const float r0 = (float)z.real(), i0 = (float)z.imag();
+  cplx best(r0, i0);
+  double err = std::fabs(std::abs(best) - target);
+  float r = r0;
+  for (int a = 0; a < 8; ++a) r = std::nextafter(r, -INFINITY);
+  for (int a = -8; a <= 8; ++a, r = std::nextafter(r, INFINITY)) {
+    float im = i0;
+    for (int b = 0; b < 8; ++b) im = std::nextafter(im, -INFINITY);
+    for (int b = -8; b <= 8; ++b, im = std::nextafter(im, INFINITY)) {
+      const cplx c((double)r, (double)im);
+      const double e = std::fabs(std::abs(c) - target);
+      if (e < err) {
+        err = e;
+        best = c;
+      }
+    }
+  }
+  return best;
+}
+
 // Appends the op of lowered gate L (register positions: target / first
 // qubit p0, control / second qubit p1) and multiplies kappa by the scalar
 // factored out.  Returns false for items the engine does not run (gradient
 // reductions, misordered quads).
 inline bool factor_gate(const Lowered& L, int R, int p0, int p1, std::vector<GxOp>* out,
-                        cplx* kappa) {
+                        cplx* kappa, bool f32 = false) {
   auto coef = [&](int i) { return cplx(L.m[2 * i], L.m[2 * i + 1]); };
+  // scalar of a rotation-like shear with exact coefficient t, rounded to tr:
+  // s * sqrt(1 + t^2) / sqrt(1 + tr^2) keeps s [[1, tr], [-tr, 1]] unitary
+  // whenever s [[1, t], [-t, 1]] was
+  auto shear_scale = [&](double s, double t, double tr) {
+    return s * std::sqrt(1.0 + t * t) / std::sqrt(1.0 + tr * tr);
+  };
   const cplx one(1.0, 0.0), zero(0.0, 0.0);
   GxOp op;
   switch (L.shape) {
@@ -158,7 +199,7 @@ inline bool factor_gate(const Lowered& L, int R, int p0, int p1, std::vector<GxO
         } else {
           op.code = code1(R, G_PHASE, p0);
           op.ncoef = 1;
-          op.c[0] = (a == one) ? d : d / a;
+          op.c[0] = unit_round((a == one) ? d : d / a, f32);
           *kappa *= a;
         }
       } else if (is_real(a) && is_real(b) && is_real(c) && is_real(d)) {
@@ -170,14 +211,18 @@ inline bool factor_gate(const Lowered& L, int R, int p0, int p1, std::vector<GxO
                    std::fabs(ar) >= std::fabs(cr)) {
           op.code = code1(R, G_SHEAR, p0);
           op.ncoef = 1;
-          op.c[0] = cplx(br / ar, cr / ar);
-          *kappa *= ar;
+          const double t1 = br / ar, t2 = cr / ar;
+          const double r1 = round_to(t1, f32), r2 = round_to(t2, f32);
+          op.c[0] = cplx(r1, r2);
+          *kappa *= (br == -cr) ? shear_scale(ar, t1, r1) : ar;
         } else if (cr != 0.0 && br == -cr && std::fabs(cr) >= std::fabs(ar) &&
                    std::fabs(cr) >= std::fabs(dr)) {
           op.code = code1(R, G_SHEARO, p0);
           op.ncoef = 1;
-          op.c[0] = cplx(ar / cr, dr / cr);
-          *kappa *= cr;
+          const double g1 = ar / cr, g2 = dr / cr;
+          const double r1 = round_to(g1, f32), r2 = round_to(g2, f32);
+          op.c[0] = cplx(r1, r2);
+          *kappa *= (ar == dr) ? shear_scale(cr, g1, r1) : cr;
         } else {
           op.code = code1(R, G_REAL2, p0);
           op.ncoef = 2;
@@ -189,16 +234,20 @@ inline bool factor_gate(const Lowered& L, int R, int p0, int p1, std::vector<GxO
                  std::fabs(a.real()) >= std::fabs(c.imag())) {
         op.code = code1(R, G_ISHEAR, p0);
         op.ncoef = 1;
-        op.c[0] = cplx(b.imag() / a.real(), c.imag() / a.real());
-        *kappa *= a.real();
+        const double t1 = b.imag() / a.real(), t2 = c.imag() / a.real();
+        const double r1 = round_to(t1, f32), r2 = round_to(t2, f32);
+        op.c[0] = cplx(r1, r2);
+        *kappa *= (b == c) ? shear_scale(a.real(), t1, r1) : a.real();
       } else if (is_real(a) && is_real(d) && is_imag(b) && is_imag(c) && b == c &&
                  b.imag() != 0.0 && std::fabs(b.imag()) >= std::fabs(a.real()) &&
                  std::fabs(b.imag()) >= std::fabs(d.real())) {
         const double s = -b.imag();
         op.code = code1(R, G_ISHEARO, p0);
         op.ncoef = 1;
-        op.c[0] = cplx(a.real() / s, d.real() / s);
-        *kappa *= s;
+        const double g1 = a.real() / s, g2 = d.real() / s;
+        const double r1 = round_to(g1, f32), r2 = round_to(g2, f32);
+        op.c[0] = cplx(r1, r2);
+        *kappa *= (a == d) ? shear_scale(s, g1, r1) : s;
       } else {
         op.code = code1(R, G_GEN2, p0);
         op.ncoef = 4;
@@ -213,7 +262,7 @@ inline bool factor_gate(const Lowered& L, int R, int p0, int p1, std::vector<GxO
       } else {
         op.code = code1(R, G_PHASE, p0);
         op.ncoef = 1;
-        op.c[0] = l;
+        op.c[0] = unit_round(l, f32);
       }
       break;
     }
@@ -225,7 +274,7 @@ inline bool factor_gate(const Lowered& L, int R, int p0, int p1, std::vector<GxO
         op.code = code2(R, d == -one ? G_CNEG : G_CPH, p0, p1, L.cval);
         if (d != -one) {
           op.ncoef = 1;
-          op.c[0] = d;
+          op.c[0] = unit_round(d, f32);
         }
       } else {
         op.code = code2(R, G_CGEN2, p0, p1, L.cval);
@@ -241,7 +290,7 @@ inline bool factor_gate(const Lowered& L, int R, int p0, int p1, std::vector<GxO
       } else {
         op.code = code2(R, G_CPH, p0, p1, L.cval);
         op.ncoef = 1;
-        op.c[0] = l;
+        op.c[0] = unit_round(l, f32);
       }
       break;
     }
@@ -250,7 +299,7 @@ inline bool factor_gate(const Lowered& L, int R, int p0, int p1, std::vector<GxO
       if (L.mul) {
         op.code = code4(R, G_ISWAP, p0, p1);
         op.ncoef = 1;
-        op.c[0] = coef(0);
+        op.c[0] = unit_round(coef(0), f32);
       } else {
         op.code = code4(R, G_SWAP, p0, p1);
       }
@@ -434,6 +483,8 @@ inline bool pack_gate_plan(const std::vector<Lowered>& gates, int n, int m, int 
   const std::vector<Stage> stages =
       plan_stages(gates, n, m, low, max_gates, two_vector ? kMaxStageRed : 0, plan_cap,
                   elem_bytes);
+  const bool f32 = elem_bytes == 8;  // complex<float>: coefficients applied in float
+  cplx carry(1.0, 0.0);  // rounding error of the stage scales so far (error feedback)
   std::vector<GxOp> ops;
   for (const Stage& stg : stages) {
     GxStage gs;
@@ -484,13 +535,16 @@ inline bool pack_gate_plan(const std::vector<Lowered>& gates, int n, int m, int 
         const bool one = L.shape == SH_PAIR || L.shape == SH_HALF;
         const int r0 = reg_of[local_of[L.t0]];
         const int r1 = one ? 0 : reg_of[local_of[L.t1]];
-        if (!factor_gate(L, R, r0, r1, &ops, &kappa)) return false;
+        if (!factor_gate(L, R, r0, r1, &ops, &kappa, f32)) return false;
       }
       if (pi + 1 == pl.size() && kappa != cplx(1.0, 0.0)) {
         GxOp sc;
         sc.code = code_scale(R);
         sc.ncoef = 1;
-        sc.c[0] = kappa;
+        const cplx want = kappa * carry;
+        const cplx got(round_to(want.real(), f32), round_to(want.imag(), f32));
+        sc.c[0] = got;
+        if (got != cplx(0.0, 0.0)) carry = want / got;
         ops.push_back(sc);
       }
       gp.op0 = (int32_t)(out->ops.size() - gs.op0);
