@@ -155,20 +155,28 @@ typedef struct qsv_fuse_opts {
   int reg_bits;      /* k: qubits per register block inside a tile           */
   int max_stage_gates;
   int profile;       /* 1: time every stage with CUDA events (see below)   */
-  int engine;        /* complex single-vector sweeps: 0 (default) = every
-                        register pass of 3 tile bits multiplied out into an
-                        8x8 complex matrix in FP64 and applied on the FP64
-                        tensor cores (mma.sync f64), complex<float> states
-                        rounded once per pass;
+  int engine;        /* complex single-vector sweeps:
+                        0 (default) = 5 for complex<float>, 2 for
+                        complex<double>;
                         1 = sparse register passes on the CUDA cores;
-                        2 = same as 0;
+                        2 = every register pass of 3 tile bits multiplied
+                        out into an 8x8 complex matrix in FP64 and applied
+                        on the FP64 tensor cores (mma.sync f64),
+                        complex<float> states rounded once per pass;
                         3 = complex<float>: TF32 three-term split on tcgen05
                         with the state rows in tensor memory (tiles of
                         2^10 .. 2^13 amplitudes, else as 4);
                         4 = complex<float>: TF32 three-term split on
-                        mma.sync.  The TF32 engines are faster but their
-                        FP32 accumulation truncates: the norm shrinks by
-                        about 1e-7 per pass.                               */
+                        mma.sync (the TF32 engines' FP32 accumulation
+                        truncates: the norm shrinks by about 1e-7 per pass);
+                        5 = gate-specialised register passes: every gate is
+                        one op whose register positions are compile-time,
+                        one-qubit gates factored to two multiply-adds per
+                        component with their scalar applied once per stage,
+                        in the state's precision (reg_bits 4, or 5 for
+                        complex<float>, the default there).
+                        Two-vector (adjoint) sweeps use 5 unless 1 is
+                        asked for.                                           */
   int ctas_per_sm;   /* engine 5: resident CTAs per SM the stage kernel is
                         built for (0 = default; 2 or 3)                    */
   int reserved;

@@ -475,7 +475,8 @@ int gate_pass_bits(size_t elem_bytes, const qsv_fuse_opts* opts, int nv) {
   // two vectors: 3 bits (complex<double>) or 4 (complex<float>); one vector:
   // 4 bits, or 5 for complex<float> with reg_bits = 5
   if (nv == 2) return elem_bytes >= 16 ? 3 : 4;
-  return (elem_bytes < 16 && opts && opts->reg_bits == 5) ? 5 : 4;
+  if (elem_bytes >= 16) return 4;
+  return (opts && opts->reg_bits == 4) ? 4 : 5;
 }
 
 namespace {

@@ -89,7 +89,7 @@ def test_fused_matches_reference_within_tolerance(states, dtype):
         # specialised passes of 4 bits, or 5 for complex<float>)
         for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=2), L.FuseOpts(engine=3),
                      L.FuseOpts(engine=4), L.FuseOpts(engine=5),
-                     L.FuseOpts(engine=5, reg_bits=5),
+                     L.FuseOpts(engine=5, reg_bits=4),
                      L.FuseOpts(engine=5, tile_bits=6, low_bits=1),
                      L.FuseOpts(engine=5, tile_bits=12, low_bits=5, max_stage_gates=3),
                      L.FuseOpts(tile_bits=10, low_bits=3, engine=3),
@@ -116,7 +116,7 @@ def test_random_mixed_large(states, dtype, n):
         y = run_gpu(states, n, dtype, recs, op, 0, x)
         assert np.array_equal(y, ref)
         for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=2), L.FuseOpts(engine=3),
-                     L.FuseOpts(engine=4), L.FuseOpts(engine=5), L.FuseOpts(engine=5, reg_bits=5)):
+                     L.FuseOpts(engine=4), L.FuseOpts(engine=5), L.FuseOpts(engine=5, reg_bits=4)):
             yf = run_gpu(states, n, dtype, recs, op, 0, x, fused=True, opts=opts)
             assert np.max(np.abs(yf - ref)) <= tol(dtype), (op, opts and opts.engine)
 
@@ -154,7 +154,7 @@ def test_complex_float_fused_keeps_the_norm(states):
     x[0] = 1
     ref = run_gpu(states, n, np.complex128, r128, "N", 0, x, fused=True)
     for opts, bound in ((None, 1e-6), (L.FuseOpts(engine=4), 1e-3), (L.FuseOpts(engine=5), 1e-6),
-                        (L.FuseOpts(engine=5, reg_bits=5), 1e-6)):
+                        (L.FuseOpts(engine=5, reg_bits=4), 1e-6)):
         y = run_gpu(states, n, np.complex64, r128, "N", 0, x.astype(np.complex64), fused=True,
                     opts=opts).astype(np.complex128)
         infid = 1.0 - abs(np.vdot(ref, y)) ** 2
@@ -174,7 +174,7 @@ def test_fused_small_states_and_empty_lists(states, dtype):
         x /= np.linalg.norm(x)
         ref = oracle.apply(x.copy(), recs, "N")
         for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=3), L.FuseOpts(engine=4),
-                     L.FuseOpts(engine=5), L.FuseOpts(engine=5, reg_bits=5)):
+                     L.FuseOpts(engine=5), L.FuseOpts(engine=5, reg_bits=4)):
             y = run_gpu(states, n, dtype, recs, "N", 0, x, fused=True, opts=opts)
             assert np.max(np.abs(y - ref)) <= tol(dtype), (n, opts and opts.engine)
         for fused in (False, True):

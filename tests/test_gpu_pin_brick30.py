@@ -72,7 +72,7 @@ def test_fused_complex_double_within_1e12(reference_state):
 
 def test_fused_complex_float_within_1e5(reference_state):
     ref, recs = reference_state
-    for opts in (None, L.FuseOpts(engine=5), L.FuseOpts(engine=5, reg_bits=5)):
+    for opts in (None, L.FuseOpts(engine=5), L.FuseOpts(engine=5, reg_bits=4)):
         with StateVector(N, np.complex64) as f:
             f.apply(recs, "N", 0, fused=True, opts=opts)
             ip, maxabs = f.compare(ref)
