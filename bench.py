@@ -158,8 +158,9 @@ def precision_extra(torch, stream, n=32, depth=100, seed=11):
         c128_ms = timed(lambda: d.apply(r128, "N", 0, fused=True))
         d_norm2 = d.norm2()
         zd = d.expectation(zz)
-        engines = [("default", None), ("gates_r4", L.FuseOpts(engine=5)),
-                   ("gates_r5", L.FuseOpts(engine=5, reg_bits=5)),
+        engines = [("default (gate passes, 5 bits)", None),
+                   ("gate passes, 4 bits", L.FuseOpts(engine=5, reg_bits=4)),
+                   ("fp64_mma", L.FuseOpts(engine=2)),
                    ("tf32_mma_sync", L.FuseOpts(engine=4))]
         runs = {}
         for name, opts in engines:
@@ -190,7 +191,7 @@ def precision_extra(torch, stream, n=32, depth=100, seed=11):
                        else 0.5) * (1 << n) * 16 for r in layer)
         unfused = {"gates": len(layer), "ms": u_ms, "gates_per_s": len(layer) / (u_ms / 1e3),
                    "hbm_gbs": u_bytes / (u_ms / 1e3) / 1e9, "path": "qsv_apply (bit-exact)"}
-    best = runs["default"]
+    best = runs["default (gate passes, 5 bits)"]
     out.update({"c64_ms": best["ms"], "c128_ms": c128_ms,
                 "c64_gates_per_s": best["gates_per_s"],
                 "c128_gates_per_s": len(r128) / (c128_ms / 1e3),

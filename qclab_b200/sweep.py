@@ -9,10 +9,11 @@ brick (default): a seeded random brick circuit (``workloads.brick``) through
 sweep; prints one JSON line with the gates, stages and tensor-core passes of
 the plan (``qsv_plan_passes``), the wall time of each sweep (host planning
 included, stream synchronised) and gates/s.  ``--engine`` is
-``qsv_fuse_opts.engine``: 0 default (FP64 MMA), 1 sparse register passes,
-2 as 0, 3 tcgen05 TF32 for complex<float>, 4 mma.sync TF32 for
-complex<float>, 5 gate-specialised register passes (``--reg-bits`` 4, or 5
-for complex<float>).
+``qsv_fuse_opts.engine``: 0 default (5 for complex<float>, 2 for
+complex<double>), 1 sparse register passes, 2 FP64 MMA dense passes, 3
+tcgen05 TF32 for complex<float>, 4 mma.sync TF32 for complex<float>, 5
+gate-specialised register passes (``--reg-bits`` 4, or 5 for
+complex<float>).
 
 adjoint: energy and full gradient (``qsv_adjoint_gradient``) of the
 hardware-efficient ansatz ``workloads.hea(qubits, depth)`` for
