@@ -466,8 +466,9 @@ def run_reference_arm(args, rank, world):
 
 
 def full_size_parity(torch, stream, n, args, recs, sv):
-    """Parity of this step's fused complex<double> state `sv` (and of a fused
-    complex<float> sweep) against the reference-exact path; the latter is
+    """Parity of the fused complex<double> sweep (run again in the bench's
+    state `sv`) and of a fused complex<float> sweep against the
+    reference-exact path; the latter is
     checked against the committed summary of QCLAB++'s CPU simulate on the
     same circuit (tests/golden/make_brick30_pin.py) when that fixture exists
     for this workload."""
@@ -492,15 +493,10 @@ def full_size_parity(torch, stream, n, args, recs, sv):
         else:
             out.update({"against": "qsv_apply (bitwise equal to QCLAB++ CPU apply in tests)",
                         "bitwise": None})
-        if len(sub) < len(recs):  # else `sv` holds the fused state of the whole circuit
-            fused = StateVector(n, np.complex128)
-            fused.set_stream(stream.cuda_stream)
-            fused.apply(sub, "N", 0, fused=True)
-        else:
-            fused = None
-        ip, maxabs = (fused or sv).compare(ref)
-        if fused is not None:
-            fused.close()
+        # the fused complex<double> sweep of the same gates, in the bench's state
+        sv.set_basis(0)
+        sv.apply(sub, "N", 0, fused=True)
+        ip, maxabs = sv.compare(ref)
         out["c128_fused"] = {"max_abs_error": maxabs, "infidelity": 1.0 - abs(ip) ** 2,
                              "bound": 1e-12}
         with StateVector(n, np.complex64) as f:
