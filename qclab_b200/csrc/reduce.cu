@@ -21,16 +21,36 @@
 namespace qsv {
 namespace {
 
+__host__ __device__ inline size_t fx_align16(size_t b) { return (b + 15) & ~size_t(15); }
+
 constexpr int kRedThreads = 512;
 constexpr int kRedBlocks = 148 * 8;
 
 struct DTerm {
   uint32_t flip_local;
-  uint32_t pad;
+  uint32_t zy_local;  // the tile bits of zy, as local bits (tiled groups)
   uint64_t flip;   // global flip mask
   uint64_t zy;     // global sign mask
   double wr, wi;   // coef * i^ny
 };
+
+// A term as a tile group's kernels stage it in shared memory: its sign on
+// the tile's fixed bits, parity((base ^ flip) & zy), folded into the weight,
+// so the sign of local element e is that weight times (-1)^popc(e & zy_local)
+// -- no global index per element and term.
+struct STerm {
+  uint32_t flip_local, zy_local;
+  double wr, wi;
+};
+
+__device__ __forceinline__ void stage_terms(STerm* ts, const DTerm* __restrict__ terms, int nterms,
+                                            uint64_t base) {
+  for (int t = threadIdx.x; t < nterms; t += blockDim.x) {
+    const DTerm T = terms[t];
+    const bool odd = __popcll((base ^ T.flip) & T.zy) & 1;
+    ts[t] = STerm{T.flip_local, T.zy_local, odd ? -T.wr : T.wr, odd ? -T.wi : T.wi};
+  }
+}
 
 template <typename V>
 __global__ void __launch_bounds__(kRedThreads)
@@ -95,27 +115,26 @@ k_expect(const V* __restrict__ st, TileArgs ta, const DTerm* __restrict__ terms,
          double2* __restrict__ partial) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* tile = reinterpret_cast<V*>(smem_raw);
-  __shared__ double2 red[32];
   const uint32_t size = 1u << ta.m;
+  STerm* ts = reinterpret_cast<STerm*>(smem_raw + fx_align16(size_t(size) * sizeof(V)));
+  __shared__ double2 red[32];
   const uint64_t base = tile_base(ta, blockIdx.x);
   for (uint32_t e = threadIdx.x; e < size; e += blockDim.x)
     tile[e] = st[tile_global(ta, ta.runoff, base, e)];
+  stage_terms(ts, terms, nterms, base);
   __syncthreads();
+  // sum_t w_t sum_e conj(x_e) (-1)^popc(e & zy_t) x_{e ^ f_t}
   double2 acc = make_double2(0.0, 0.0);
-  for (int t = 0; t < nterms; ++t) {
-    const DTerm T = terms[t];
-    double2 s = make_double2(0.0, 0.0);
-    for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) {
-      const uint64_t g = tile_global(ta, ta.runoff, base, e);
-      const double2 x = to_d2(tile[e]);
+  for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) {
+    const double2 x = to_d2(tile[e]);
+    for (int t = 0; t < nterms; ++t) {
+      const STerm T = ts[t];
       const double2 y = to_d2(tile[e ^ T.flip_local]);
-      const double sg = sgn_of((g ^ T.flip) & T.zy);
-      // conj(x) * y * sg
-      s.x = fma(sg * x.x, y.x, fma(sg * x.y, y.y, s.x));
-      s.y = fma(sg * x.x, y.y, fma(-sg * x.y, y.x, s.y));
+      const double re = fma(x.x, y.x, x.y * y.y), im = fma(x.x, y.y, -x.y * y.x);
+      const double sg = (__popc(e & T.zy_local) & 1) ? -1.0 : 1.0;
+      acc.x = fma(sg * T.wr, re, fma(-sg * T.wi, im, acc.x));
+      acc.y = fma(sg * T.wr, im, fma(sg * T.wi, re, acc.y));
     }
-    acc.x += T.wr * s.x - T.wi * s.y;
-    acc.y += T.wr * s.y + T.wi * s.x;
   }
   const double2 r = block_sum(acc, red);
   if (threadIdx.x == 0) partial[blockIdx.x] = r;
@@ -129,17 +148,19 @@ k_observable(const V* __restrict__ src, V* __restrict__ dst, TileArgs ta,
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* tile = reinterpret_cast<V*>(smem_raw);
   const uint32_t size = 1u << ta.m;
+  STerm* ts = reinterpret_cast<STerm*>(smem_raw + fx_align16(size_t(size) * sizeof(V)));
   const uint64_t base = tile_base(ta, blockIdx.x);
   for (uint32_t e = threadIdx.x; e < size; e += blockDim.x)
     tile[e] = src[tile_global(ta, ta.runoff, base, e)];
+  stage_terms(ts, terms, nterms, base);
   __syncthreads();
   for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) {
     const uint64_t g = tile_global(ta, ta.runoff, base, e);
     double2 acc = accumulate ? to_d2(dst[g]) : make_double2(0.0, 0.0);
     for (int t = 0; t < nterms; ++t) {
-      const DTerm T = terms[t];
+      const STerm T = ts[t];
       const double2 y = to_d2(tile[e ^ T.flip_local]);
-      const double sg = sgn_of((g ^ T.flip) & T.zy);
+      const double sg = (__popc(e & T.zy_local) & 1) ? -1.0 : 1.0;
       acc.x = fma(sg * T.wr, y.x, fma(-sg * T.wi, y.y, acc.x));
       acc.y = fma(sg * T.wr, y.y, fma(sg * T.wi, y.x, acc.y));
     }
@@ -301,8 +322,10 @@ qsv_status run_tiled(qsv_state_s* s, const V* src, V* dst, const std::vector<HTe
     for (int ti : G.terms) {
       const HTerm& h = T[ti];
       DTerm d{};
-      for (int b = 0; b < n; ++b)
+      for (int b = 0; b < n; ++b) {
         if ((h.flip >> b) & 1ull) d.flip_local |= 1u << local_of[b];
+        if (((h.zy >> b) & 1ull) && local_of[b] >= 0) d.zy_local |= 1u << local_of[b];
+      }
       d.flip = h.flip;
       d.zy = h.zy;
       // coef * i^ny
@@ -333,7 +356,11 @@ qsv_status run_tiled(qsv_state_s* s, const V* src, V* dst, const std::vector<HTe
                                                   cudaMemcpyHostToDevice, s->stream),
                                   "observable upload"))
     return st;
-  const size_t smem = (size_t(1) << m) * sizeof(V);
+  size_t max_terms = 0;
+  for (const Group& G : groups) max_terms = std::max(max_terms, G.terms.size());
+  const size_t smem = fx_align16((size_t(1) << m) * sizeof(V)) + max_terms * sizeof(STerm);
+  if (smem > 200 * 1024)
+    return fail(QSV_ERROR_SIZE, "observable group of %zu terms exceeds shared memory", max_terms);
   auto kern_e = k_expect<V>;
   auto kern_o = k_observable<V>;
   if (qsv_status st = cuda_status(cudaFuncSetAttribute(expect ? (const void*)kern_e : (const void*)kern_o,
