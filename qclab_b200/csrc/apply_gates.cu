@@ -398,6 +398,12 @@ __global__ void __launch_bounds__(NT, MINB) k_gates(V* __restrict__ v0, V* __res
         }
       }
       for (int o = 0; o < nops; ++o) apply_word<V, R, NV>(x, y, ops[op0 + o], coefs, racc, lanes);
+      // the store recomputes the offsets: without this the compiler keeps
+      // all 2^R of them live across the ops for reuse, which costs registers
+      // the amplitudes need
+      asm volatile("" : "+r"(ptb));
+#pragma unroll
+      for (int k = 0; k < R; ++k) asm volatile("" : "+r"(boff[k]));
       if (pairs) {
 #pragma unroll
         for (int j = 0; j < N; j += 2) {
@@ -431,8 +437,7 @@ __global__ void __launch_bounds__(NT, MINB) k_gates(V* __restrict__ v0, V* __res
 // for complex<double> with R = 4, whose op switch needs ~190 registers in
 // all), so single-vector complex<double> runs CTAs of 128 threads, two per
 // SM by default (three with qsv_fuse_opts.ctas_per_sm = 3, at 168
-// registers; R = 3: four per SM at 126 registers); complex<float> with R = 4
-// runs 256-thread CTAs, three per SM
+// registers); complex<float> with R = 4 runs 256-thread CTAs, three per SM
 // (two on request), with R = 5 two 128-thread CTAs.  Two-vector sweeps hold
 // 2 x 2^R amplitudes: R = 3 for complex<double>, 4 for complex<float>, in
 // 128-thread CTAs, two per SM.  Each thread takes ngroups / threads
@@ -441,7 +446,6 @@ template <typename V> struct GxKernels;
 template <> struct GxKernels<double2> {
   static void* get(int R, int ctas, int nv) {
     if (nv == 2) return (void*)k_gates<double2, 3, 128, 2, 2>;
-    if (R == 3) return (void*)k_gates<double2, 3, 128, 4, 1>;
     return ctas == 3 ? (void*)k_gates<double2, 4, 128, 3, 1>
                      : (void*)k_gates<double2, 4, 128, 2, 1>;
   }
@@ -476,7 +480,7 @@ int gate_pass_bits(size_t elem_bytes, const qsv_fuse_opts* opts, int nv) {
   // two vectors: 3 bits (complex<double>) or 4 (complex<float>); one vector:
   // 4 bits, or 5 for complex<float> with reg_bits = 5
   if (nv == 2) return elem_bytes >= 16 ? 3 : 4;
-  if (elem_bytes >= 16) return (opts && opts->reg_bits == 3) ? 3 : 4;
+  if (elem_bytes >= 16) return 4;
   return (opts && opts->reg_bits == 4) ? 4 : 5;
 }
 

@@ -48,9 +48,9 @@ class StageTimer {
 // with nothing launched, when the items do not fit it.
 template <typename V>
 qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool vec16);
-// Register bits of its passes: single-vector 4 for 16-byte elements (3 with
-// qsv_fuse_opts.reg_bits = 3), 5 for 8-byte ones (4 with reg_bits = 4);
-// two-vector 3 (16-byte) or 4 (8-byte).
+// Register bits of its passes: single-vector 4 for 16-byte elements, 5 for
+// 8-byte ones (4 with qsv_fuse_opts.reg_bits = 4); two-vector 3 (16-byte)
+// or 4 (8-byte).
 int gate_pass_bits(size_t elem_bytes, const qsv_fuse_opts* opts, int nv = 1);
 // Fixed-order sum of x.partial's rows (x.nslots rows of ntiles tile sums)
 // into x.rows_out, on the state's stream.
