@@ -440,12 +440,12 @@ __global__ void __launch_bounds__(NT, MINB) k_gates(V* __restrict__ v0, V* __res
 // registers); complex<float> with R = 4 runs 256-thread CTAs, three per SM
 // (two on request), with R = 5 two 128-thread CTAs.  Two-vector sweeps hold
 // 2 x 2^R amplitudes: R = 3 for complex<double>, 4 for complex<float>, in
-// 128-thread CTAs, two per SM.  Each thread takes ngroups / threads
+// 128-thread CTAs, three per SM (166 registers).  Each thread takes ngroups / threads
 // register groups per pass.
 template <typename V> struct GxKernels;
 template <> struct GxKernels<double2> {
   static void* get(int R, int ctas, int nv) {
-    if (nv == 2) return (void*)k_gates<double2, 3, 128, 2, 2>;
+    if (nv == 2) return (void*)k_gates<double2, 3, 128, 3, 2>;
     return ctas == 3 ? (void*)k_gates<double2, 4, 128, 3, 1>
                      : (void*)k_gates<double2, 4, 128, 2, 1>;
   }
@@ -453,7 +453,7 @@ template <> struct GxKernels<double2> {
 };
 template <> struct GxKernels<float2> {
   static void* get(int R, int ctas, int nv) {
-    if (nv == 2) return (void*)k_gates<float2, 4, 128, 2, 2>;
+    if (nv == 2) return (void*)k_gates<float2, 4, 128, 3, 2>;
     if (R == 5) return (void*)k_gates<float2, 5, 128, 2, 1>;
     return ctas == 2 ? (void*)k_gates<float2, 4, 256, 2, 1> : (void*)k_gates<float2, 4, 256, 3, 1>;
   }
