@@ -118,6 +118,9 @@ const char* qsv_last_error(void);
 const char* qsv_status_string(qsv_status status);
 /* number of kernel launches this library has issued on the calling thread */
 uint64_t    qsv_launch_count(void);
+/* of those, stage launches whose tiles moved between global and shared
+ * memory by TMA (cp.async.bulk.tensor)                                     */
+uint64_t    qsv_tma_launch_count(void);
 
 /* ---- state vectors ------------------------------------------------------ */
 /* Allocates a 2^nbQubits state on the current device, set to |0...0>.
@@ -179,7 +182,11 @@ typedef struct qsv_fuse_opts {
                         asked for.                                           */
   int ctas_per_sm;   /* engine 5: resident CTAs per SM the stage kernel is
                         built for (0 = default; 2 or 3)                    */
-  int reserved;
+  int tile_copy;     /* engine 5: how tiles move between global and shared
+                        memory: 0 (default) = TMA (cp.async.bulk.tensor,
+                        one thread per CTA, 128-byte swizzle) wherever the
+                        stage's tile fits a 5-D tensor map, else 1;
+                        1 = 16-byte cp.async by every thread              */
 } qsv_fuse_opts;
 
 /* Fused path: the gate list is planned into stages; each stage streams the

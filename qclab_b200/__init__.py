@@ -14,6 +14,6 @@ from .gates import (QObject, QGate1, QGate2, QControlledGate2, Identity, Hadamar
                     RotationYY, RotationZZ, MatrixGate2, ControlledGate, CX, CNOT, CY, CZ,
                     CPhase, CRotationX, CRotationY, CRotationZ)
 from .circuit import QCircuit
-from .state import StateVector, launch_count
+from .state import StateVector, launch_count, tma_launch_count
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -52,7 +52,7 @@ class FuseOpts(C.Structure):
     """``qsv_fuse_opts``."""
     _fields_ = [("tile_bits", C.c_int), ("low_bits", C.c_int), ("reg_bits", C.c_int),
                 ("max_stage_gates", C.c_int), ("profile", C.c_int), ("engine", C.c_int),
-                ("ctas_per_sm", C.c_int), ("reserved", C.c_int)]
+                ("ctas_per_sm", C.c_int), ("tile_copy", C.c_int)]
 
 
 class BatchOpts(C.Structure):
@@ -90,6 +90,7 @@ def _declare(lib):
         "qsv_last_error": ([], C.c_char_p),
         "qsv_status_string": ([i], C.c_char_p),
         "qsv_launch_count": ([], C.c_uint64),
+        "qsv_tma_launch_count": ([], C.c_uint64),
         "qsv_create": ([i, i, C.POINTER(p)], i),
         "qsv_wrap": ([i, i, p, C.POINTER(p)], i),
         "qsv_destroy": ([p], i),

@@ -11,6 +11,7 @@ namespace qsv {
 
 static thread_local char g_err[1024] = "";
 static thread_local uint64_t g_launches = 0;
+static thread_local uint64_t g_tma_launches = 0;
 
 void set_error(const char* fmt, ...) {
   va_list ap;
@@ -34,6 +35,7 @@ qsv_status cuda_status(cudaError_t e, const char* what) {
 }
 
 void count_launch(uint64_t k) { g_launches += k; }
+void count_tma_launch() { ++g_tma_launches; }
 
 qsv_status stream_wait(cudaStream_t waiter, cudaStream_t producer) {
   if (waiter == producer) return QSV_SUCCESS;
@@ -158,6 +160,8 @@ int qsv_abi_version(void) { return QSV_ABI_VERSION; }
 const char* qsv_last_error(void) { return g_err; }
 
 uint64_t qsv_launch_count(void) { return g_launches; }
+
+uint64_t qsv_tma_launch_count(void) { return g_tma_launches; }
 
 const char* qsv_status_string(qsv_status status) {
   switch (status) {

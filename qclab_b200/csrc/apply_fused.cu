@@ -15,6 +15,7 @@
 // gates, which changes rounding).
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <array>
 #include <complex>
 #include <initializer_list>
@@ -1368,6 +1369,17 @@ int effective_tile_bits(size_t eb, int nv, int n, const qsv_fuse_opts* opts) {
 }
 int default_low_bits(size_t eb) { return eb >= 16 ? 2 : 3; }
 
+unsigned* sweep_wait_flag() {
+  static unsigned* addr = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_tc_status) == cudaSuccess) addr = static_cast<unsigned*>(p);
+  });
+  if (addr) g_tc_used = true;
+  return addr;
+}
+
 qsv_status tc_check_status(cudaStream_t stream) {
   if (!g_tc_used.load(std::memory_order_relaxed)) return QSV_SUCCESS;
   unsigned v = 0;
@@ -1381,7 +1393,9 @@ qsv_status tc_check_status(cudaStream_t stream) {
   static const unsigned zero = 0;
   cudaMemcpyToSymbolAsync(g_tc_status, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, stream);
   cudaStreamSynchronize(stream);
-  return fail(QSV_ERROR_TIMEOUT, "a tensor-core sweep gave up waiting for its MMAs (results invalid)");
+  return fail(QSV_ERROR_TIMEOUT,
+              "a fused sweep gave up waiting for its MMAs or tile copies, or found a tile copy "
+              "outside its shared memory (results invalid)");
 }
 
 qsv_status execute_fused(const ExecArgs& x) {

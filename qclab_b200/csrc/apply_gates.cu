@@ -23,6 +23,7 @@
 #include "fused.hpp"
 #include "gate_plan.hpp"
 #include "stage_exec.cuh"
+#include "tma.cuh"
 #include "gate_cases.inc"
 
 namespace qsv {
@@ -326,7 +327,13 @@ struct GxArgs {
   int nred;
   const int32_t* red_slots;
   double* partial;
+  // tile staging by TMA (tma.use; maps passed beside) or 16-byte cp.async
+  TmaGeo tma;
+  unsigned* wait_error;  // set when a bounded wait for the tile gave up
+  uint32_t smem_bytes;   // dynamic shared memory of the launch
 };
+
+constexpr int kTileWaitLimit = 2000;  // suspended polls (up to 1 ms each) for a tile load
 
 template <int R>
 __device__ __forceinline__ uint32_t reg_off(uint32_t ptb, const uint32_t (&boff)[R], int j) {
@@ -338,9 +345,14 @@ __device__ __forceinline__ uint32_t reg_off(uint32_t ptb, const uint32_t (&boff)
 }
 
 template <typename V, int R, int NT, int MINB, int NV>
-__global__ void __launch_bounds__(NT, MINB) k_gates(V* __restrict__ v0, V* __restrict__ v1,
-                                                    GxArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(NT, MINB)
+    k_gates(V* __restrict__ v0, V* __restrict__ v1, GxArgs a,
+            const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1) {
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  __shared__ uint64_t tile_bar;
+  // the tiles start on a 1024-byte boundary (the TMA swizzle blocks; the
+  // launch reserves the padding)
+  unsigned char* smem_raw = smem_dyn + ((1024u - (tc::smem_addr(smem_dyn) & 1023u)) & 1023u);
   const uint32_t size = 1u << a.ta.m;
   V* t0 = reinterpret_cast<V*>(smem_raw);
   V* t1 = t0 + size;
@@ -351,6 +363,35 @@ __global__ void __launch_bounds__(NT, MINB) k_gates(V* __restrict__ v0, V* __res
   unsigned char* pp = smem_raw + size_t(NV) * size * sizeof(V) + (NV == 2 ? fx::kRaccBytes : 0);
   unsigned char* po = pp + align16(size_t(a.npasses) * sizeof(GxPassDev));
   unsigned char* pc = po + align16(size_t(a.nops) * sizeof(uint32_t));
+  const uint64_t base = tile_base(a.ta, blockIdx.x);
+  const uint32_t copies = 1u << a.tma.nit;
+  if (a.tma.use) {
+    // the copies must land inside this launch's shared memory, on 1024-byte
+    // boundaries; otherwise the tile is left alone and the sweep reports it
+    const uint32_t off = tc::smem_addr(t0) - tc::smem_addr(smem_dyn);
+    const bool fits = (tc::smem_addr(t0) & 1023u) == 0 && (a.tma.box_bytes & 1023u) == 0 &&
+                      copies * a.tma.box_bytes == size * sizeof(V) &&
+                      off + uint64_t(NV) * copies * a.tma.box_bytes <= a.smem_bytes;
+    if (!fits) {
+      if (threadIdx.x == 0) atomicOr(a.wait_error, 2u);
+      return;
+    }
+  }
+  if (a.tma.use) {  // one thread starts the tile's copies; they land while the plan is copied
+    if (threadIdx.x == 0) {
+      tc::bar_init(&tile_bar, 1);
+      tc::bar_init_fence();
+      tma::expect_tx(&tile_bar, copies * a.tma.box_bytes * NV);
+      for (uint32_t i = 0; i < copies; ++i) {
+        int c[5];
+        tma::coords(a.tma, tma::copy_word(a.tma, base, i), c);
+        tma::load(reinterpret_cast<unsigned char*>(t0) + i * a.tma.box_bytes, &tm0, c, &tile_bar);
+        if (NV == 2)
+          tma::load(reinterpret_cast<unsigned char*>(t1) + i * a.tma.box_bytes, &tm1, c,
+                    &tile_bar);
+      }
+    }
+  }
   copy_words(pp, a.passes, size_t(a.npasses) * sizeof(GxPassDev));
   copy_words(po, a.ops, size_t(a.nops) * sizeof(uint32_t));
   copy_words(pc, a.coefs, size_t(a.ncoef) * sizeof(V));
@@ -359,9 +400,22 @@ __global__ void __launch_bounds__(NT, MINB) k_gates(V* __restrict__ v0, V* __res
   const GxPassDev* passes = reinterpret_cast<const GxPassDev*>(pp);
   const uint32_t* ops = reinterpret_cast<const uint32_t*>(po);
   const V* coefs = reinterpret_cast<const V*>(pc);
-  const uint64_t base = tile_base(a.ta, blockIdx.x);
-  load_tile<V, NV>(v0, v1, t0, t1, a.ta, base, a.vec16);
-  __syncthreads();
+  if (a.tma.use) {
+    // the barrier's initialisation is visible to the other threads after
+    // this barrier; the tile after its phase completes
+    __syncthreads();
+    const bool ok = tma::wait_phase(&tile_bar, 0, kTileWaitLimit);
+    if (__syncthreads_or(!ok)) {  // give up: flag it, let the copies drain, leave the tile
+      if (threadIdx.x == 0) {
+        atomicOr(a.wait_error, 1u);
+        (void)tma::wait_phase(&tile_bar, 0, kTileWaitLimit);
+      }
+      return;
+    }
+  } else {
+    load_tile<V, NV>(v0, v1, t0, t1, a.ta, base, a.vec16);
+    __syncthreads();
+  }
   constexpr int N = 1 << R;
   const uint32_t ngroups = size >> R;
   const unsigned lanes = blockDim.x < 32u ? blockDim.x : 32u;
@@ -422,7 +476,23 @@ __global__ void __launch_bounds__(NT, MINB) k_gates(V* __restrict__ v0, V* __res
     }
     __syncthreads();
   }
-  store_tile<V, NV>(v0, v1, t0, t1, a.ta, base, a.vec16);
+  if (a.tma.use) {
+    // the passes' shared-memory writes, then one thread copies the tile out
+    tc::fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (uint32_t i = 0; i < copies; ++i) {
+        int c[5];
+        tma::coords(a.tma, tma::copy_word(a.tma, base, i), c);
+        tma::store(&tm0, c, reinterpret_cast<const unsigned char*>(t0) + i * a.tma.box_bytes);
+        if (NV == 2)
+          tma::store(&tm1, c, reinterpret_cast<const unsigned char*>(t1) + i * a.tma.box_bytes);
+      }
+      tma::store_commit_and_wait();
+    }
+  } else {
+    store_tile<V, NV>(v0, v1, t0, t1, a.ta, base, a.vec16);
+  }
   if (NV == 2) {  // the last pass ended with a barrier: racc is complete
     const int warps = fx::red_warps();
     for (int r = threadIdx.x; r < a.nred; r += blockDim.x) {
@@ -510,10 +580,31 @@ qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool 
   if (nv == 2 && x.nslots > 0 && x.partial_bytes < (size_t)x.nslots * (1ull << (n - m)) * sizeof(double))
     return fail(QSV_ERROR_SIZE, "partial-sum buffer too small");
   if (plan.stages.empty()) return QSV_SUCCESS;
+  // tile staging per stage: TMA maps where the tile fits one (both vectors
+  // share the geometry), else cp.async; the shared-memory layout, and so the
+  // passes' offsets, follow the choice
+  const bool want_tma = !(x.opts && x.opts->tile_copy == 1);
+  std::vector<CUtensorMap> maps(plan.stages.size() * 2);
+  std::vector<TmaGeo> geos(plan.stages.size());
+  for (size_t si = 0; si < plan.stages.size(); ++si) {
+    const GxStage& gs = plan.stages[si];
+    geos[si] = TmaGeo{};
+    if (!want_tma) continue;
+    if (!tma_stage_map(gs.bits, gs.m, n, sizeof(V), x.v0, &maps[2 * si], &geos[si])) continue;
+    if (nv == 2 && !tma_stage_map(gs.bits, gs.m, n, sizeof(V), x.v1, &maps[2 * si + 1],
+                                  &geos[si]))
+      geos[si] = TmaGeo{};
+  }
   std::vector<GxPassDev> dpass(plan.passes.size());
   std::vector<uint64_t> runoff;
   std::vector<size_t> run0;
-  for (const GxStage& gs : plan.stages) {
+  for (size_t si = 0; si < plan.stages.size(); ++si) {
+    const GxStage& gs = plan.stages[si];
+    const bool tma = geos[si].use != 0;
+    auto phys = [&](uint32_t e) {
+      return tma ? phys_tma_host(e, fx::Units<V>::per, geos[si].swz)
+                 : fx::phys_host(e, fx::Units<V>::per);
+    };
     for (size_t pi = gs.pass0; pi < gs.pass0 + gs.npasses; ++pi) {
       const GxPass& gp = plan.passes[pi];
       GxPassDev& d = dpass[pi];
@@ -521,13 +612,13 @@ qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool 
       for (int k = 0; k < 8; ++k) d.pos[k] = gp.pos[k];
       d.op0 = gp.op0;
       d.nops = gp.nops;
-      for (int k = 0; k < R; ++k) d.boff[k] = fx::phys_host(1u << gp.pos[k], fx::Units<V>::per);
+      for (int k = 0; k < R; ++k) d.boff[k] = phys(1u << gp.pos[k]);
       int order[32];
       int pos[8];
       for (int k = 0; k < 8; ++k) pos[k] = gp.pos[k];
-      const int ng = lane_order(pos, R, gs.m, sizeof(V), order);
+      const int ng = lane_order(pos, R, gs.m, sizeof(V), order, tma ? geos[si].swz : -1);
       if (ng > 12) return fail(QSV_ERROR_SIZE, "gate stage of %d tile bits", gs.m);
-      for (int k = 0; k < ng; ++k) d.goff[k] = fx::phys_host(1u << order[k], fx::Units<V>::per);
+      for (int k = 0; k < ng; ++k) d.goff[k] = phys(1u << order[k]);
     }
     run0.push_back(runoff.size());
     tile_runoffs(gs.bits, gs.m, low, &runoff);
@@ -566,6 +657,8 @@ qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool 
   if (x.ntiles_out) *x.ntiles_out = ntiles;
   const unsigned threads =
       (unsigned)std::min<uint64_t>((uint64_t)GxKernels<V>::threads(R, nv), 1ull << (m - R));
+  unsigned* wait_error = sweep_wait_flag();
+  if (!wait_error) return fail(QSV_ERROR_CUDA, "sweep wait flag unavailable");
   StageTimer timer(x.opts && x.opts->profile, plan.stages.size(), s->stream);
   if (qsv_status st = timer.start()) return st;
   V* p0 = static_cast<V*>(x.v0);
@@ -588,16 +681,21 @@ qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool 
     a.ops = reinterpret_cast<const uint32_t*>(dev + op_off) + gs.op0;
     a.coefs = dev + coef_off + gs.coef0 * sizeof(V);
     a.vec16 = vec16 ? 1 : 0;
+    a.tma = geos[si];
+    a.wait_error = wait_error;
+    // + 1024: the tiles are placed on a 1024-byte boundary
     const size_t smem = (size_t(1) << gs.m) * sizeof(V) * nv + (nv == 2 ? fx::kRaccBytes : 0) +
-                        gx_plan_smem<V>(gs.npasses, gs.nops, gs.ncoef);
+                        gx_plan_smem<V>(gs.npasses, gs.nops, gs.ncoef) + 1024;
     if (smem > 200 * 1024)
       return fail(QSV_ERROR_SIZE, "gate stage needs %zu bytes of shared memory", smem);
-    void* args[] = {&p0, &p1, &a};
+    a.smem_bytes = (uint32_t)smem;
+    void* args[] = {&p0, &p1, &a, &maps[2 * si], &maps[2 * si + (nv == 2 ? 1 : 0)]};
     if (qsv_status st = cuda_status(cudaLaunchKernel(kern, dim3((unsigned)ntiles), dim3(threads),
                                                      args, smem, s->stream),
                                     "gate stage launch"))
       return st;
     count_launch();
+    if (a.tma.use) count_tma_launch();
     if (qsv_status st = timer.mark(si)) return st;
   }
   if (qsv_status st = timer.finish()) return st;

@@ -68,6 +68,10 @@ qsv_status execute_fused(const ExecArgs& x);
 // gave up since the last call; reads the device flag on `stream` (call after
 // that stream has synchronised; nothing is read before a tcgen05 launch).
 qsv_status tc_check_status(cudaStream_t stream);
+// Device flag that a sweep kernel sets when one of its bounded waits gave
+// up (read and cleared by tc_check_status at the next synchronisation);
+// null if its address cannot be had.
+unsigned* sweep_wait_flag();
 
 // Tile bits the executor uses for nv vectors of an n-qubit state: the
 // requested (or default) size, at most 14 and n, and at most 256 threads of

@@ -427,21 +427,29 @@ inline void host_apply_op2(cplx* x, cplx* y, int R, uint32_t word, const cplx* c
 // 16-byte accesses (complex<double>, or complex<float> pairs when tile bit 0
 // is a pass bit) or 16 lanes of 8-byte accesses: their 3 (or 4) lowest g
 // bits should map to tile bits whose slot bits are distinct.
-inline int lane_order(const int* pos, int R, int m, size_t elem_bytes, int* order) {
+// `tma_swz` >= 0 selects the TMA layout instead (tma.cuh: u -> u ^ ((u >> 3)
+// & (2^B - 1)), B = tma_swz): unit bits 0-2 are slot bits 0-2, unit bits
+// 3 .. 3+B-1 fold into slot bits 0 .. B-1, the others give no distinct slot.
+inline int lane_order(const int* pos, int R, int m, size_t elem_bytes, int* order,
+                      int tma_swz = -1) {
   uint32_t pass = 0;
   for (int k = 0; k < R; ++k) pass |= 1u << pos[k];
   std::vector<int> rest;
   for (int b = 0; b < m; ++b)
     if (!((pass >> b) & 1u)) rest.push_back(b);
   const bool pairs = elem_bytes == 8 && (pass & 1u);
-  auto slot = [&](int b) { return elem_bytes >= 16 ? b % 3 : (b - 1) % 3; };
+  auto slot = [&](int b) {
+    const int ub = elem_bytes >= 16 ? b : b - 1;  // unit bit
+    if (tma_swz < 0) return ub % 3;
+    return ub < 3 ? ub : (ub - 3 < tma_swz ? ub - 3 : -1);
+  };
   std::vector<int> first;
   if (elem_bytes == 8 && !pairs && !rest.empty() && rest[0] == 0) first.push_back(0);
   bool used[3] = {false, false, false};
   for (int b : rest) {
     if (b == 0 && elem_bytes == 8) continue;
     const int sl = slot(b);
-    if (!used[sl]) {
+    if (sl >= 0 && !used[sl]) {
       used[sl] = true;
       first.push_back(b);
     }

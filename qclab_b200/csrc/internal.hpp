@@ -27,6 +27,8 @@ void set_error(const char* fmt, ...);
 qsv_status fail(qsv_status st, const char* fmt, ...);
 qsv_status cuda_status(cudaError_t e, const char* what);
 void count_launch(uint64_t k = 1);
+// one stage launch whose tiles move by TMA
+void count_tma_launch();
 // Makes `waiter` wait (on the device, no host synchronisation) for the work
 // issued to `producer` so far; a no-op for the same stream.
 qsv_status stream_wait(cudaStream_t waiter, cudaStream_t producer);

@@ -176,6 +176,11 @@ def launch_count() -> int:
     return int(L.load().qsv_launch_count())
 
 
+def tma_launch_count() -> int:
+    """Stage launches on this thread whose tiles moved by TMA."""
+    return int(L.load().qsv_tma_launch_count())
+
+
 def _obs_args(obs):
     from .observable import Observable
     if not isinstance(obs, Observable):

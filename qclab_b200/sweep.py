@@ -61,6 +61,8 @@ def main(argv=None, keep_state: bool = False) -> dict:
     p.add_argument("--low-bits", type=int, default=0)
     p.add_argument("--reg-bits", type=int, default=0)
     p.add_argument("--ctas-per-sm", type=int, default=0)
+    p.add_argument("--tile-copy", type=int, default=0,
+                   help="engine 5 tile staging: 0 = TMA where possible, 1 = cp.async")
     p.add_argument("--repeat", type=int, default=2)
     p.add_argument("--workload", choices=["brick", "adjoint", "batch", "kernels"],
                    default="brick")
@@ -75,14 +77,15 @@ def main(argv=None, keep_state: bool = False) -> dict:
     dt, code = DTYPES[a.dtype]
     recs = W.brick(a.qubits, a.depth, seed=a.seed).gate_records(dt)
     opts = L.FuseOpts(engine=a.engine, tile_bits=a.tile_bits, low_bits=a.low_bits,
-                      reg_bits=a.reg_bits, ctas_per_sm=a.ctas_per_sm)
+                      reg_bits=a.reg_bits, ctas_per_sm=a.ctas_per_sm, tile_copy=a.tile_copy)
     lib = L.load()
     arr, ptr, cnt = L.gate_array(recs)
     ns, npas, nops = C.c_int(), C.c_int(), C.c_int()
     L.check(lib.qsv_plan_passes(a.qubits, code, ptr, cnt, b"N", 0, C.byref(opts), C.byref(ns),
                                 C.byref(npas), C.byref(nops)), "qsv_plan_passes")
     out = {"qubits": a.qubits, "depth": a.depth, "dtype": a.dtype, "engine": a.engine,
-           "gates": int(cnt), "stages": ns.value, "passes": npas.value}
+           "tile_copy": a.tile_copy, "gates": int(cnt), "stages": ns.value,
+           "passes": npas.value}
     ms = []
     with StateVector(a.qubits, dt) as s:
         s.apply(recs, "N", 0, fused=True, opts=opts)

@@ -121,6 +121,52 @@ def test_random_mixed_large(states, dtype, n):
             assert np.max(np.abs(yf - ref)) <= tol(dtype), (op, opts and opts.engine)
 
 
+def scattered_circuit(n, seed):
+    """Gates on every other qubit above the low three, so a stage's tile bits
+    form many runs (more than the five dimensions of one tensor map)."""
+    from qclab_b200 import gates as G
+    from qclab_b200.circuit import QCircuit
+    rng = np.random.default_rng(seed)
+    c = QCircuit(n)
+    spread = list(range(4, n, 2))
+    for layer in range(3):
+        for q in [0, 1, 2] + spread:
+            c.push_back(G.RotationY(q, float(rng.uniform(0, 6.28))))
+            c.push_back(G.RotationZ(q, float(rng.uniform(0, 6.28))))
+        for a, b in zip(spread, spread[1:]):
+            c.push_back(G.CNOT(a, b) if layer % 2 else G.CZ(a, b))
+        c.push_back(G.CNOT(2, spread[0]))
+    return c
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=lambda d: np.dtype(d).name)
+@pytest.mark.parametrize("n,tile_bits,low_bits,kind", [
+    (13, 10, 2, "mixed"), (17, 12, 3, "mixed"), (19, 11, 1, "mixed"), (21, 12, 5, "mixed"),
+    (18, 10, 3, "scattered"), (20, 11, 3, "scattered"), (16, 12, 2, "scattered")])
+def test_gate_engine_tma_staging(states, dtype, n, tile_bits, low_bits, kind):
+    """Engine 5 with its tiles moved by TMA (5-D tensor maps over the tile's
+    bit runs, one copy per value of the bits past the fifth run, 128-byte
+    swizzle) against the oracle and against the same plan staged with
+    cp.async."""
+    from qclab_b200 import tma_launch_count
+    rng = np.random.default_rng(n + tile_bits)
+    c = W.random_mixed(n, 150, seed=n + 7) if kind == "mixed" else scattered_circuit(n, n)
+    recs = c.gate_records(dtype)
+    x = (rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)).astype(dtype)
+    x /= np.linalg.norm(x)
+    ref = oracle.apply(x.copy(), recs, "N")
+    opts = dict(engine=5, tile_bits=tile_bits, low_bits=low_bits)
+    before = tma_launch_count()
+    y_tma = run_gpu(states, n, dtype, recs, "N", 0, x, fused=True, opts=L.FuseOpts(**opts))
+    assert tma_launch_count() > before  # the stages' tiles moved by TMA
+    mid = tma_launch_count()
+    y_cp = run_gpu(states, n, dtype, recs, "N", 0, x, fused=True,
+                   opts=L.FuseOpts(**opts, tile_copy=1))
+    assert tma_launch_count() == mid
+    assert np.max(np.abs(y_tma - ref)) <= tol(dtype)
+    assert np.max(np.abs(y_cp - ref)) <= tol(dtype)
+
+
 @pytest.mark.parametrize("tile_bits", [10, 11, 12, 13])
 def test_tcgen05_tiles(states, tile_bits):
     """complex<float> sweeps on tcgen05 (engine 3): tiles of 1 to 8 M = 128
