@@ -27,6 +27,7 @@
 #include "fused.hpp"
 #include "stage_exec.cuh"
 #include "tcgen05.cuh"
+#include "tma.cuh"
 
 namespace qsv {
 
@@ -461,6 +462,10 @@ struct DmmaArgs {
   const POp* ops;
   const double2* coefs;  // per pass: U column-major (U[i][k] at k * 4 + i)
   int vec16;
+  // k_dmma3: tile staging by TMA (tma.use, map passed beside) or cp.async
+  TmaGeo tma;
+  unsigned* wait_error;
+  uint32_t smem_bytes;
 };
 
 template <typename V>
@@ -529,18 +534,30 @@ __global__ void __launch_bounds__(256, 3) k_dmma(V* __restrict__ v0, DmmaArgs a)
 // same output amplitude q for groups 2k4 and 2k4 + 1: 32 MMAs per chunk of
 // 32 groups x 8 amplitudes, one 16-byte store per output.
 template <typename V>
-__global__ void __launch_bounds__(256, 2) k_dmma3(V* __restrict__ v0, DmmaArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(256, 2)
+    k_dmma3(V* __restrict__ v0, DmmaArgs a, const __grid_constant__ CUtensorMap tm0) {
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  __shared__ uint64_t tile_bar;
+  unsigned char* smem_raw = tma::align1024(smem_dyn);  // the launch reserves the padding
   const uint32_t size = 1u << a.ta.m;
   V* t0 = reinterpret_cast<V*>(smem_raw);
+  const uint64_t base = tile_base(a.ta, blockIdx.x);
+  if (a.tma.use) {  // one thread starts the tile's copies; they land while the plan is copied
+    if (!tma::tile_fits<1>(a.tma, smem_dyn, t0, size * sizeof(V), a.smem_bytes, a.wait_error))
+      return;
+    tma::tile_start<1>(a.tma, &tm0, &tm0, t0, nullptr, base, &tile_bar);
+  }
   const PassDev* passes;
   const POp* ops;
   const double2* coefs;
   stage_plan<double2>(smem_raw + size_t(size) * sizeof(V), a.passes, a.npasses, a.ops, a.nops,
                       a.coefs, a.ncoef, &passes, &ops, &coefs);
-  const uint64_t base = tile_base(a.ta, blockIdx.x);
-  load_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
-  __syncthreads();
+  if (a.tma.use) {
+    if (!tma::tile_wait(&tile_bar, a.wait_error, tma::kTileWaitLimit)) return;
+  } else {
+    load_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
+    __syncthreads();
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int q = lane >> 2, k4 = lane & 3;
   const uint32_t nchunks = size >> 8;  // 32 groups x 8 amplitudes
@@ -613,7 +630,10 @@ __global__ void __launch_bounds__(256, 2) k_dmma3(V* __restrict__ v0, DmmaArgs a
     }
     __syncthreads();
   }
-  store_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
+  if (a.tma.use)
+    tma::tile_store<1>(a.tma, &tm0, &tm0, t0, nullptr, base);
+  else
+    store_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
 }
 
 // complex<float> passes of three tile bits on the TF32 tensor cores with the
@@ -906,20 +926,24 @@ int gf2_rank(std::initializer_list<uint32_t> in) {
 // so that the shared-memory banks a quarter-warp (16-byte elements) or
 // half-warp (8-byte elements) touches on load and on store are independent
 // of the banks of the pass bits p0, p1 that vary within it.
-void dmma_tables_compute(PassDev* P, int R, int m, int epu);
+// swz < 0: the cp.async layout (phys_host); swz >= 0: a TMA-staged tile
+// whose swizzle has XOR width swz (phys_tma_host).
+void dmma_tables_compute(PassDev* P, int R, int m, int epu, int swz);
 
-// The tables depend only on (pass bits, tile bits, element size); passes of
-// a circuit repeat a few patterns, so they are cached per host thread.
-void dmma_tables(PassDev* P, int R, int m, int epu) {
+// The tables depend only on (pass bits, tile bits, element size, layout);
+// passes of a circuit repeat a few patterns, so they are cached per host
+// thread.
+void dmma_tables(PassDev* P, int R, int m, int epu, int swz) {
   thread_local std::unordered_map<uint64_t, std::array<uint16_t, 32>> cache;
   const uint64_t key = (uint64_t)(uint8_t)P->pos[0] | ((uint64_t)(uint8_t)P->pos[1] << 8) |
                        ((uint64_t)(uint8_t)(R == 3 ? P->pos[2] : 0xff) << 16) |
-                       ((uint64_t)m << 24) | ((uint64_t)epu << 32) | ((uint64_t)R << 40);
+                       ((uint64_t)m << 24) | ((uint64_t)epu << 32) | ((uint64_t)R << 40) |
+                       ((uint64_t)(swz + 1) << 44);
   auto it = cache.find(key);
   if (it == cache.end()) {
     if (cache.size() > 4096) cache.clear();
     PassDev tmp = *P;
-    dmma_tables_compute(&tmp, R, m, epu);
+    dmma_tables_compute(&tmp, R, m, epu, swz);
     std::array<uint16_t, 32> t;
     std::memcpy(t.data(), tmp.off, sizeof(tmp.off));
     it = cache.emplace(key, t).first;
@@ -927,11 +951,14 @@ void dmma_tables(PassDev* P, int R, int m, int epu) {
   std::memcpy(P->off, it->second.data(), sizeof(P->off));
 }
 
-void dmma_tables_compute(PassDev* P, int R, int m, int epu) {
+void dmma_tables_compute(PassDev* P, int R, int m, int epu, int swz) {
   const int nb = R;
   int pos[3] = {P->pos[0], P->pos[1], R == 3 ? P->pos[2] : -1};
   const uint32_t bank_mask = epu == 1 ? 7u : 15u;
-  auto dir = [&](int b) { return (uint32_t)phys_host(1u << b, (uint32_t)epu) & bank_mask; };
+  auto phys = [&](uint32_t e) {
+    return swz < 0 ? phys_host(e, (uint32_t)epu) : phys_tma_host(e, (uint32_t)epu, swz);
+  };
+  auto dir = [&](int b) { return phys(1u << b) & bank_mask; };
   std::vector<int> rest;
   for (int b = 0; b < m; ++b)
     if (b != pos[0] && b != pos[1] && b != pos[2]) rest.push_back(b);
@@ -957,7 +984,7 @@ void dmma_tables_compute(PassDev* P, int R, int m, int epu) {
       if ((g >> i) & 1u) e |= 1u << sel[i];
     return e;
   };
-  auto ph = [&](uint32_t e) { return (uint16_t)phys_host(e, (uint32_t)epu); };
+  auto ph = [&](uint32_t e) { return (uint16_t)phys(e); };
   for (int t = 0; t < 4; ++t) P->off[t] = ph(map(8u * t));
   for (int g = 0; g < 8; ++g) P->off[4 + g] = ph(map((uint32_t)g));
   const int na = 1 << nb;
@@ -1108,7 +1135,9 @@ qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool v
   const int R = dmma_pass_bits(m);
   PackedPlan<double2> plan;
   // plans sized per launch: a few KB typically, at most kDmmaPlanMax
-  if ((size_t(1) << m) * sizeof(V) + kDmmaPlanMax > 200 * 1024) return QSV_ERROR_NOT_SUPPORTED;
+  // (+ 1024: k_dmma3 aligns its tile to 1024 bytes)
+  if ((size_t(1) << m) * sizeof(V) + kDmmaPlanMax + 1024 > 200 * 1024)
+    return QSV_ERROR_NOT_SUPPORTED;
   const bool low_fixed = x.opts && x.opts->low_bits > 0;
   if (qsv_status st = pack_dense_plan(*x.items, n, m, low, low_fixed, R, max_gates, sizeof(V), &plan,
                                       &low))
@@ -1124,7 +1153,19 @@ qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool v
   const bool f32 = std::is_same<V, float2>::value && R == 3;
   const bool tcg = f32 && engine == 3 && m >= 10 && m <= 13;
   const bool tf32 = f32 && (engine == 4 || engine == 3);
-  for (const PackedStage& ps : plan.stages)
+  // k_dmma3 tiles move by TMA where the stage's tile fits a tensor map
+  // (qsv_fuse_opts.tile_copy = 1: cp.async)
+  const bool dmma3 = !tcg && !tf32 && R == 3;
+  const bool want_tma = dmma3 && !(x.opts && x.opts->tile_copy == 1);
+  std::vector<CUtensorMap> maps(plan.stages.size());
+  std::vector<TmaGeo> geos(plan.stages.size());
+  for (size_t si = 0; si < plan.stages.size(); ++si) {
+    geos[si] = TmaGeo{};
+    const PackedStage& ps = plan.stages[si];
+    if (want_tma) tma_stage_map(ps.bits, ps.m, n, sizeof(V), x.v0, &maps[si], &geos[si]);
+  }
+  for (size_t si = 0; si < plan.stages.size(); ++si) {
+    const PackedStage& ps = plan.stages[si];
     for (size_t pi = ps.pass0; pi < ps.pass0 + ps.npasses; ++pi) {
       PassDev& P = plan.passes[pi];
       if (P.nops != 1 || plan.ops[ps.op0 + P.op0].shape != P_DENSE || ps.m < 5 + R ||
@@ -1133,8 +1174,11 @@ qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool v
       if (tcg)
         tc_tables(&P, ps.m);
       else
-        dmma_tables(&P, R, ps.m, Units<V>::per);
+        dmma_tables(&P, R, ps.m, Units<V>::per, geos[si].use ? geos[si].swz : -1);
     }
+  }
+  unsigned* wait_error = sweep_wait_flag();
+  if (dmma3 && !wait_error) return fail(QSV_ERROR_CUDA, "sweep wait flag unavailable");
   auto align = [](size_t v) { return (v + 255) & ~size_t(255); };
   const size_t pass_bytes = plan.passes.size() * sizeof(PassDev);
   const size_t op_off = align(pass_bytes);
@@ -1184,17 +1228,25 @@ qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool v
     a.ops = reinterpret_cast<const POp*>(dev + op_off) + ps.op0;
     a.coefs = reinterpret_cast<const double2*>(dev + coef_off) + ps.coef0;
     a.vec16 = vec16 ? 1 : 0;
+    a.tma = geos[si];
+    a.wait_error = wait_error;
+    // k_dmma3: + 1024 for its tile's 1024-byte alignment
     const size_t smem_stage =
         tcg ? std::max(kTcMinSmem, (size_t(1) << ps.m) * sizeof(V) + 4096 + 128 +
                                        plan_smem_bytes<double2>((int)ps.npasses, ps.nops, 0))
             : (size_t(1) << ps.m) * sizeof(V) +
-                  plan_smem_bytes<double2>((int)ps.npasses, ps.nops, ps.ncoef);
-    void* args[] = {&p0, &a};
+                  plan_smem_bytes<double2>((int)ps.npasses, ps.nops, ps.ncoef) +
+                  (dmma3 ? 1024 : 0);
+    a.smem_bytes = (uint32_t)smem_stage;
+    void* args2[] = {&p0, &a};
+    void* args3[] = {&p0, &a, &maps[si]};
+    void** args = dmma3 ? args3 : args2;
     if (qsv_status st = cuda_status(cudaLaunchKernel(kern, dim3((unsigned)ntiles),
                                                      dim3(256), args, smem_stage, s->stream),
                                     "dense stage launch"))
       return st;
     count_launch();
+    if (a.tma.use) count_tma_launch();
     if (profile) cudaEventRecord(ev[si + 1], s->stream);
   }
   if (profile) {
@@ -1239,8 +1291,9 @@ qsv_status execute_typed(const ExecArgs& x) {
   if constexpr (Elem<V>::cplx) {
     if (x.nv == 1 && x.nslots == 0 && use_gate_engine<V>(opts)) {
       const int mg = gate_tile_bits<V>(n, opts);
+      const int lowg = (opts && opts->low_bits > 0) ? low : gate_default_low(sizeof(V));
       if (mg > 0) {
-        const qsv_status st = execute_gates<V>(x, mg, std::min(low, mg), max_gates, vec16);
+        const qsv_status st = execute_gates<V>(x, mg, std::min(lowg, mg), max_gates, vec16);
         if (st != QSV_ERROR_NOT_SUPPORTED) return st;
       }
     }
@@ -1369,6 +1422,11 @@ int effective_tile_bits(size_t eb, int nv, int n, const qsv_fuse_opts* opts) {
 }
 int default_low_bits(size_t eb) { return eb >= 16 ? 2 : 3; }
 
+// complex<float> gate passes keep 4 low bits unless told otherwise: a
+// 128-byte innermost TMA box and fewer passes (30-qubit brick, depth 40:
+// 166 passes in 503 ms against 192 passes in 528 ms with 3 low bits)
+int gate_default_low(size_t eb) { return eb == 8 ? 4 : default_low_bits(eb); }
+
 unsigned* sweep_wait_flag() {
   static unsigned* addr = nullptr;
   static std::once_flag once;
@@ -1439,7 +1497,7 @@ qsv_status plan_counts(const std::vector<Lowered>& low, int n, const qsv_fuse_op
     const int mg = use_gate_engine<V>(opts) ? gate_tile_bits<V>(n, opts) : -1;
     if (mg > 0) {
       const int lowb = std::min((opts && opts->low_bits > 0) ? opts->low_bits
-                                                             : default_low_bits(sizeof(V)), mg);
+                                                             : gate_default_low(sizeof(V)), mg);
       const int max_gates = (opts && opts->max_stage_gates > 0) ? opts->max_stage_gates : 256;
       std::vector<int> o, p;
       const qsv_status st = gate_plan_counts(low, n, mg, lowb, opts, max_gates, sizeof(V), &o, &p);

@@ -333,8 +333,6 @@ struct GxArgs {
   uint32_t smem_bytes;   // dynamic shared memory of the launch
 };
 
-constexpr int kTileWaitLimit = 2000;  // suspended polls (up to 1 ms each) for a tile load
-
 template <int R>
 __device__ __forceinline__ uint32_t reg_off(uint32_t ptb, const uint32_t (&boff)[R], int j) {
   uint32_t o = ptb;
@@ -352,7 +350,7 @@ __global__ void __launch_bounds__(NT, MINB)
   __shared__ uint64_t tile_bar;
   // the tiles start on a 1024-byte boundary (the TMA swizzle blocks; the
   // launch reserves the padding)
-  unsigned char* smem_raw = smem_dyn + ((1024u - (tc::smem_addr(smem_dyn) & 1023u)) & 1023u);
+  unsigned char* smem_raw = tma::align1024(smem_dyn);
   const uint32_t size = 1u << a.ta.m;
   V* t0 = reinterpret_cast<V*>(smem_raw);
   V* t1 = t0 + size;
@@ -364,33 +362,10 @@ __global__ void __launch_bounds__(NT, MINB)
   unsigned char* po = pp + align16(size_t(a.npasses) * sizeof(GxPassDev));
   unsigned char* pc = po + align16(size_t(a.nops) * sizeof(uint32_t));
   const uint64_t base = tile_base(a.ta, blockIdx.x);
-  const uint32_t copies = 1u << a.tma.nit;
-  if (a.tma.use) {
-    // the copies must land inside this launch's shared memory, on 1024-byte
-    // boundaries; otherwise the tile is left alone and the sweep reports it
-    const uint32_t off = tc::smem_addr(t0) - tc::smem_addr(smem_dyn);
-    const bool fits = (tc::smem_addr(t0) & 1023u) == 0 && (a.tma.box_bytes & 1023u) == 0 &&
-                      copies * a.tma.box_bytes == size * sizeof(V) &&
-                      off + uint64_t(NV) * copies * a.tma.box_bytes <= a.smem_bytes;
-    if (!fits) {
-      if (threadIdx.x == 0) atomicOr(a.wait_error, 2u);
-      return;
-    }
-  }
   if (a.tma.use) {  // one thread starts the tile's copies; they land while the plan is copied
-    if (threadIdx.x == 0) {
-      tc::bar_init(&tile_bar, 1);
-      tc::bar_init_fence();
-      tma::expect_tx(&tile_bar, copies * a.tma.box_bytes * NV);
-      for (uint32_t i = 0; i < copies; ++i) {
-        int c[5];
-        tma::coords(a.tma, tma::copy_word(a.tma, base, i), c);
-        tma::load(reinterpret_cast<unsigned char*>(t0) + i * a.tma.box_bytes, &tm0, c, &tile_bar);
-        if (NV == 2)
-          tma::load(reinterpret_cast<unsigned char*>(t1) + i * a.tma.box_bytes, &tm1, c,
-                    &tile_bar);
-      }
-    }
+    if (!tma::tile_fits<NV>(a.tma, smem_dyn, t0, size * sizeof(V), a.smem_bytes, a.wait_error))
+      return;
+    tma::tile_start<NV>(a.tma, &tm0, &tm1, t0, t1, base, &tile_bar);
   }
   copy_words(pp, a.passes, size_t(a.npasses) * sizeof(GxPassDev));
   copy_words(po, a.ops, size_t(a.nops) * sizeof(uint32_t));
@@ -401,17 +376,7 @@ __global__ void __launch_bounds__(NT, MINB)
   const uint32_t* ops = reinterpret_cast<const uint32_t*>(po);
   const V* coefs = reinterpret_cast<const V*>(pc);
   if (a.tma.use) {
-    // the barrier's initialisation is visible to the other threads after
-    // this barrier; the tile after its phase completes
-    __syncthreads();
-    const bool ok = tma::wait_phase(&tile_bar, 0, kTileWaitLimit);
-    if (__syncthreads_or(!ok)) {  // give up: flag it, let the copies drain, leave the tile
-      if (threadIdx.x == 0) {
-        atomicOr(a.wait_error, 1u);
-        (void)tma::wait_phase(&tile_bar, 0, kTileWaitLimit);
-      }
-      return;
-    }
+    if (!tma::tile_wait(&tile_bar, a.wait_error, tma::kTileWaitLimit)) return;
   } else {
     load_tile<V, NV>(v0, v1, t0, t1, a.ta, base, a.vec16);
     __syncthreads();
@@ -477,19 +442,7 @@ __global__ void __launch_bounds__(NT, MINB)
     __syncthreads();
   }
   if (a.tma.use) {
-    // the passes' shared-memory writes, then one thread copies the tile out
-    tc::fence_proxy_async();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (uint32_t i = 0; i < copies; ++i) {
-        int c[5];
-        tma::coords(a.tma, tma::copy_word(a.tma, base, i), c);
-        tma::store(&tm0, c, reinterpret_cast<const unsigned char*>(t0) + i * a.tma.box_bytes);
-        if (NV == 2)
-          tma::store(&tm1, c, reinterpret_cast<const unsigned char*>(t1) + i * a.tma.box_bytes);
-      }
-      tma::store_commit_and_wait();
-    }
+    tma::tile_store<NV>(a.tma, &tm0, &tm1, t0, t1, base);
   } else {
     store_tile<V, NV>(v0, v1, t0, t1, a.ta, base, a.vec16);
   }

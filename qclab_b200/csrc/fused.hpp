@@ -60,6 +60,8 @@ qsv_status gate_plan_counts(const std::vector<Lowered>& items, int n, int m, int
                             const qsv_fuse_opts* opts, int max_gates, size_t elem_bytes,
                             std::vector<int>* ops, std::vector<int>* passes);
 int default_low_bits(size_t elem_bytes);
+// low bits of complex single-vector gate-pass sweeps (engine 5) when unset
+int gate_default_low(size_t elem_bytes);
 
 // Plans the items into stages and runs them.
 qsv_status execute_fused(const ExecArgs& x);

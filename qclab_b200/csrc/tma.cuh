@@ -110,6 +110,84 @@ __device__ __forceinline__ void store_commit_and_wait() {
   asm volatile("cp.async.bulk.commit_group;\ncp.async.bulk.wait_group 0;" ::: "memory");
 }
 
+// ---- one stage tile (NV vectors of tile_bytes each) ------------------------
+// The stage kernels call, in order: tile_fits (every thread; false: the
+// copies would not land inside the launch's shared memory on 1024-byte
+// boundaries -- flag 2 is set and the kernel returns), tile_start (one
+// thread initialises the mbarrier and issues the loads), their own
+// independent work, tile_wait (every thread; false: the bounded wait gave
+// up -- flag 1 is set, the copies are given time to drain, the kernel
+// returns), the passes, tile_store (every thread; one issues the stores and
+// waits for them).
+
+template <int NV>
+__device__ __forceinline__ bool tile_fits(const TmaGeo& g, const void* smem_dyn, const void* t0,
+                                          uint32_t tile_bytes, uint32_t smem_bytes,
+                                          unsigned* err) {
+  const uint32_t off = tc::smem_addr(t0) - tc::smem_addr(smem_dyn);
+  const uint32_t copies = 1u << g.nit;
+  const bool ok = (tc::smem_addr(t0) & 1023u) == 0 && (g.box_bytes & 1023u) == 0 &&
+                  copies * g.box_bytes == tile_bytes &&
+                  off + uint64_t(NV) * tile_bytes <= smem_bytes;
+  if (!ok && threadIdx.x == 0) atomicOr(err, 2u);
+  return ok;
+}
+
+template <int NV>
+__device__ __forceinline__ void tile_start(const TmaGeo& g, const CUtensorMap* m0,
+                                           const CUtensorMap* m1, void* t0, void* t1,
+                                           uint64_t base, uint64_t* bar) {
+  if (threadIdx.x != 0) return;
+  const uint32_t copies = 1u << g.nit;
+  tc::bar_init(bar, 1);
+  tc::bar_init_fence();
+  expect_tx(bar, copies * g.box_bytes * NV);
+  for (uint32_t i = 0; i < copies; ++i) {
+    int c[5];
+    coords(g, copy_word(g, base, i), c);
+    load(static_cast<unsigned char*>(t0) + i * g.box_bytes, m0, c, bar);
+    if (NV == 2) load(static_cast<unsigned char*>(t1) + i * g.box_bytes, m1, c, bar);
+  }
+}
+
+__device__ __forceinline__ bool tile_wait(uint64_t* bar, unsigned* err, int limit) {
+  __syncthreads();  // the mbarrier's initialisation, for the other threads
+  const bool ok = wait_phase(bar, 0, limit);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) {
+      atomicOr(err, 1u);
+      (void)wait_phase(bar, 0, limit);
+    }
+    return false;
+  }
+  return true;
+}
+
+template <int NV>
+__device__ __forceinline__ void tile_store(const TmaGeo& g, const CUtensorMap* m0,
+                                           const CUtensorMap* m1, const void* t0, const void* t1,
+                                           uint64_t base) {
+  tc::fence_proxy_async();  // this thread's shared-memory writes, for the copy engine
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const uint32_t copies = 1u << g.nit;
+  for (uint32_t i = 0; i < copies; ++i) {
+    int c[5];
+    coords(g, copy_word(g, base, i), c);
+    store(m0, c, static_cast<const unsigned char*>(t0) + i * g.box_bytes);
+    if (NV == 2) store(m1, c, static_cast<const unsigned char*>(t1) + i * g.box_bytes);
+  }
+  store_commit_and_wait();
+}
+
+constexpr int kTileWaitLimit = 2000;  // suspended polls (up to 1 ms each) for a tile load
+
+// Dynamic shared memory from the next 1024-byte boundary (the launch
+// reserves 1024 bytes more than it uses).
+__device__ __forceinline__ unsigned char* align1024(unsigned char* p) {
+  return p + ((1024u - (tc::smem_addr(p) & 1023u)) & 1023u);
+}
+
 }  // namespace tma
 
 // ---- host ---------------------------------------------------------------------
