@@ -39,6 +39,34 @@ struct Geo {
 template <typename V> struct M2 { V a00, a01, a10, a11; };
 template <typename V> struct M4 { V a[16]; };
 
+// Row r (0: a, 1: b) of a 2x2 gate on the pair (x1, x2), evaluated with the
+// operations of its reference lambda (lower.hpp ExactForm, apply.hpp:9-128):
+// signed zeros come out as the reference's do.  `form` is uniform per launch.
+template <typename V>
+__device__ __forceinline__ V pair_row(int form, const M2<V>& M, V x1, V x2, int r) {
+  switch (form) {
+    case EF_HADAMARD: {
+      const auto s = ere(M.a00);
+      return r ? esub(smul(s, x1), smul(s, x2)) : eadd(smul(s, x1), smul(s, x2));
+    }
+    case EF_ROTX: {
+      const auto c = ere(M.a00);
+      return r ? eadd(emul(M.a10, x1), smul(c, x2)) : eadd(smul(c, x1), emul(M.a01, x2));
+    }
+    case EF_ROTY:
+      return r ? eadd(smul(ere(M.a10), x1), smul(ere(M.a11), x2))
+               : eadd(smul(ere(M.a00), x1), smul(ere(M.a01), x2));
+    case EF_DIAG:
+      return r ? emul(M.a11, x2) : emul(M.a00, x1);
+    case EF_SWAP:
+      return r ? x1 : x2;
+    case EF_SWAP_MUL:
+      return r ? emul(M.a10, x1) : emul(M.a01, x2);
+    default:
+      return r ? eadd(emul(M.a10, x1), emul(M.a11, x2)) : eadd(emul(M.a00, x1), emul(M.a01, x2));
+  }
+}
+
 __device__ __forceinline__ uint64_t tile_base(const Geo& g, uint64_t w, int n) {
   uint64_t x = (n >= kLaneBits) ? (w << kLaneBits) : 0ull;
   if (g.nspec > 0) x = insert_zero(x, g.spec[0]);
@@ -58,7 +86,7 @@ __device__ __forceinline__ bool lane_active(const Geo& g, int lane) {
 // apply2 (apply.hpp:259-272) / apply4 controlled (apply.hpp:311-332).
 template <typename V, int ITEMS>
 __global__ void __launch_bounds__(kThreads)
-k_pair_reg(V* __restrict__ st, Geo g, int n, uint64_t tmask, M2<V> M) {
+k_pair_reg(V* __restrict__ st, Geo g, int n, uint64_t tmask, M2<V> M, int form) {
   const int lane = threadIdx.x & 31;
   const uint64_t w0 = warp_id() * ITEMS;
   const bool lok = lane_active(g, lane);
@@ -74,15 +102,15 @@ k_pair_reg(V* __restrict__ st, Geo g, int n, uint64_t tmask, M2<V> M) {
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i) {
     if (!ok[i]) continue;
-    st[idx[i]]         = eadd(emul(M.a00, x1[i]), emul(M.a01, x2[i]));
-    st[idx[i] | tmask] = eadd(emul(M.a10, x1[i]), emul(M.a11, x2[i]));
+    st[idx[i]]         = pair_row(form, M, x1[i], x2[i], 0);
+    st[idx[i] | tmask] = pair_row(form, M, x1[i], x2[i], 1);
   }
 }
 
 // ---- 2x2 on a pair whose target bit is a lane bit (bit < 5) --------------
 template <typename V, int ITEMS>
 __global__ void __launch_bounds__(kThreads)
-k_pair_lane(V* __restrict__ st, Geo g, int n, int tbit, M2<V> M) {
+k_pair_lane(V* __restrict__ st, Geo g, int n, int tbit, M2<V> M, int form) {
   const int lane = threadIdx.x & 31;
   const uint64_t w0 = warp_id() * ITEMS;
   const bool lok = lane_active(g, lane);
@@ -101,8 +129,7 @@ k_pair_lane(V* __restrict__ st, Geo g, int n, int tbit, M2<V> M) {
     const V p = shfl_xor(v[i], 1 << tbit);
     // lower lane: a = m11*x1 + m12*x2 with x1 = own, x2 = partner;
     // upper lane: b = m21*x1 + m22*x2 with x1 = partner, x2 = own.
-    const V out = upper ? eadd(emul(M.a10, p), emul(M.a11, v[i]))
-                        : eadd(emul(M.a00, v[i]), emul(M.a01, p));
+    const V out = upper ? pair_row(form, M, p, v[i], 1) : pair_row(form, M, v[i], p, 0);
     if (ok[i]) st[idx[i]] = out;
   }
 }
@@ -111,7 +138,7 @@ k_pair_lane(V* __restrict__ st, Geo g, int n, int tbit, M2<V> M) {
 // apply2b (apply.hpp:275-287), apply4b (apply.hpp:335-352).
 template <typename V, int ITEMS>
 __global__ void __launch_bounds__(kThreads)
-k_scale(V* __restrict__ st, Geo g, int n, V lam) {
+k_scale(V* __restrict__ st, Geo g, int n, V lam, int form) {
   const int lane = threadIdx.x & 31;
   const uint64_t w0 = warp_id() * ITEMS;
   const bool lok = lane_active(g, lane);
@@ -126,7 +153,7 @@ k_scale(V* __restrict__ st, Geo g, int n, V lam) {
   }
 #pragma unroll
   for (int i = 0; i < ITEMS; ++i)
-    if (ok[i]) st[idx[i]] = emul(lam, v[i]);
+    if (ok[i]) st[idx[i]] = (form == EF_NEG) ? eneg(v[i]) : emul(lam, v[i]);
 }
 
 template <typename V>
@@ -351,11 +378,13 @@ static qsv_status launch_typed(qsv_state_s* s, const Lowered& L) {
         gb.reg(L.t0);
         Geo g = gb.build();
         constexpr int I = 2;
-        k_pair_reg<V, I><<<blocks_for(g.ntiles, I), kThreads, 0, str>>>(st, g, n, 1ull << L.t0, M);
+        k_pair_reg<V, I><<<blocks_for(g.ntiles, I), kThreads, 0, str>>>(st, g, n, 1ull << L.t0, M,
+                                                                        L.form);
       } else {
         Geo g = gb.build();
         constexpr int I = 4;
-        k_pair_lane<V, I><<<blocks_for(g.ntiles, I), kThreads, 0, str>>>(st, g, n, L.t0, M);
+        k_pair_lane<V, I><<<blocks_for(g.ntiles, I), kThreads, 0, str>>>(st, g, n, L.t0, M,
+                                                                         L.form);
       }
       break;
     }
@@ -365,7 +394,8 @@ static qsv_status launch_typed(qsv_state_s* s, const Lowered& L) {
       if (L.shape == SH_CHALF) gb.fix(L.t1, L.cval);
       Geo g = gb.build();
       constexpr int I = 4;
-      k_scale<V, I><<<blocks_for(g.ntiles, I), kThreads, 0, str>>>(st, g, n, hcoef<V>(L.m, 0));
+      k_scale<V, I><<<blocks_for(g.ntiles, I), kThreads, 0, str>>>(st, g, n, hcoef<V>(L.m, 0),
+                                                                   L.form);
       break;
     }
     case SH_QUAD: {

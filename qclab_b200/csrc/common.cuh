@@ -46,6 +46,38 @@ __device__ __forceinline__ float2 eadd(float2 a, float2 b) {
 __device__ __forceinline__ double eadd(double a, double b) { return add_rn(a, b); }
 __device__ __forceinline__ float  eadd(float a, float b)   { return add_rn(a, b); }
 
+__device__ __forceinline__ double2 esub(double2 a, double2 b) {
+  return make_double2(sub_rn(a.x, b.x), sub_rn(a.y, b.y));
+}
+__device__ __forceinline__ float2 esub(float2 a, float2 b) {
+  return make_float2(sub_rn(a.x, b.x), sub_rn(a.y, b.y));
+}
+__device__ __forceinline__ double esub(double a, double b) { return sub_rn(a, b); }
+__device__ __forceinline__ float  esub(float a, float b)   { return sub_rn(a, b); }
+
+// s * x for a real scalar s (std::complex's real-scalar operator*: each
+// component times s)
+__device__ __forceinline__ double2 smul(double s, double2 x) {
+  return make_double2(mul_rn(s, x.x), mul_rn(s, x.y));
+}
+__device__ __forceinline__ float2 smul(float s, float2 x) {
+  return make_float2(mul_rn(s, x.x), mul_rn(s, x.y));
+}
+__device__ __forceinline__ double smul(double s, double x) { return mul_rn(s, x); }
+__device__ __forceinline__ float  smul(float s, float x)   { return mul_rn(s, x); }
+
+// -x (std::complex's unary minus: each component negated)
+__device__ __forceinline__ double2 eneg(double2 x) { return make_double2(-x.x, -x.y); }
+__device__ __forceinline__ float2  eneg(float2 x)  { return make_float2(-x.x, -x.y); }
+__device__ __forceinline__ double  eneg(double x)  { return -x; }
+__device__ __forceinline__ float   eneg(float x)   { return -x; }
+
+// real part of a coefficient
+__device__ __forceinline__ double ere(double2 m) { return m.x; }
+__device__ __forceinline__ float  ere(float2 m)  { return m.x; }
+__device__ __forceinline__ double ere(double m)  { return m; }
+__device__ __forceinline__ float  ere(float m)   { return m; }
+
 // ---- fast (FMA-contracted) arithmetic for the fused sweeps ----------------
 __device__ __forceinline__ double2 fmul(double2 m, double2 x) {
   return make_double2(fma(m.x, x.x, -m.y * x.y), fma(m.x, x.y, m.y * x.x));

@@ -15,11 +15,13 @@
 //   SH_SWAP  : swap (a|b1, a|c1), optionally times lambda
 //                                               apply4bc  apply.hpp:355-371
 //
-// Matrices are stored row-major as (re, im) pairs.  A generic complex 2x2
-// product m11*x1 + m12*x2 evaluated as (ac - bd, ad + bc) without FMA gives
-// the same values as every specialised reference lambda (Hadamard's real
-// scaling, RotationX's real cosine, PauliX's swap, ...), because the extra
-// products are exact zeros and IEEE addition/multiplication commute.
+// Matrices are stored row-major as (re, im) pairs.  Each PAIR/CPAIR/HALF/
+// CHALF gate also carries its lambda's arithmetic form (ExactForm): a
+// generic complex product m11*x1 + m12*x2, (ac - bd, ad + bc) without FMA,
+// has the values of every specialised lambda, but its extra 0 * x terms can
+// turn a -0 component into +0 where the lambda's own operations (Hadamard's
+// real scaling, PauliX's swap, PauliZ's negation, ...) keep the sign; the
+// kernels therefore evaluate each form as its lambda does.
 #pragma once
 
 #include <cmath>
@@ -34,6 +36,20 @@ enum Shape : int {
   SH_NONE = 0, SH_PAIR = 1, SH_HALF = 2, SH_QUAD = 3,
   SH_CPAIR = 4, SH_CHALF = 5, SH_SWAP = 6,
   SH_RED = 7   // gradient reduction w * Im(i^ny <lam| Pi P |psi>) (adjoint sweep)
+};
+
+// Arithmetic of a PAIR/CPAIR (a, b = rows 0, 1; x1, x2 = the pair) or
+// HALF/CHALF gate as its reference lambda evaluates it (apply.hpp:9-128):
+enum ExactForm : int {
+  EF_GENERAL = 0,  // a = m11*x1 + m12*x2, b = m21*x1 + m22*x2 (lambda_QGate1);
+                   // HALF: x *= lambda (Phase, Phase45, Phase90, CPhase)
+  EF_HADAMARD,     // a = s*x1 + s*x2, b = s*x1 - s*x2, s real
+  EF_ROTX,         // a = c*x1 + s*x2, b = s*x1 + c*x2, c real, s complex
+  EF_ROTY,         // a = c*x1 + s1*x2, b = s2*x1 + c*x2, all real
+  EF_DIAG,         // a = x1 * l1, b = x2 * l2 (RotationZ, CRotationZ)
+  EF_SWAP,         // a = x2, b = x1 (PauliX, CX)
+  EF_SWAP_MUL,     // a = x2 * l1, b = x1 * l2 (PauliY, CY)
+  EF_NEG           // HALF: x = -x (PauliZ, CZ)
 };
 
 // Generator of a parametric gate for the adjoint gradient:
@@ -57,6 +73,7 @@ struct Lowered {
   int cval = 1;    // control state
   int mul = 0;     // SWAP: multiply the swapped pair by lambda (iSWAP)
   int diag = 0;    // PAIR/CPAIR: matrix is diagonal (RotationZ-type)
+  int form = EF_GENERAL;  // PAIR/CPAIR/HALF/CHALF: the lambda's arithmetic
   int real = 1;    // all coefficients have zero imaginary part
   double m[32];    // row-major complex coefficients (already rounded to R)
   int qubits[2] = {-1, -1};  // qubits touched (after offset), -1 if unused
@@ -192,12 +209,14 @@ inline qsv_status lower_gate(const qsv_gate& g, char op, int offset, int n,
         A[0] = cx(s, zero); A[1] = cx(s, zero);
         A[2] = cx(s, zero); A[3] = cx(-s, zero);
         L.shape = SH_PAIR;
+        L.form = EF_HADAMARD;
         break;
       }
       case QSV_PAULI_X:  // lambda_PauliX, apply.hpp:46-52
         A[0] = cx(zero, zero); A[1] = cx(one, zero);
         A[2] = cx(one, zero);  A[3] = cx(zero, zero);
         L.shape = SH_PAIR;
+        L.form = EF_SWAP;
         break;
       case QSV_PAULI_Y: {  // lambda_PauliY, apply.hpp:56-68
         C<R> l1 = cx(zero, -one), l2 = cx(zero, one);
@@ -205,11 +224,13 @@ inline qsv_status lower_gate(const qsv_gate& g, char op, int offset, int n,
         A[0] = cx(zero, zero); A[1] = l1;
         A[2] = l2;             A[3] = cx(zero, zero);
         L.shape = SH_PAIR;
+        L.form = EF_SWAP_MUL;
         break;
       }
       case QSV_PAULI_Z:  // lambda_PauliZ + apply2b, apply.hpp:72-78
         A[0] = cx(-one, zero);
         L.shape = SH_HALF;
+        L.form = EF_NEG;
         break;
       case QSV_ROTATION_X: {  // lambda_RotationX, apply.hpp:82-95
         C<R> s = cx(zero, -sn);
@@ -217,6 +238,7 @@ inline qsv_status lower_gate(const qsv_gate& g, char op, int offset, int n,
         A[0] = cx(cs, zero); A[1] = s;
         A[2] = s;            A[3] = cx(cs, zero);
         L.shape = SH_PAIR;
+        L.form = EF_ROTX;
         break;
       }
       case QSV_ROTATION_Y: {  // lambda_RotationY, apply.hpp:99-113
@@ -225,6 +247,7 @@ inline qsv_status lower_gate(const qsv_gate& g, char op, int offset, int n,
         A[0] = cx(cs, zero); A[1] = cx(s1, zero);
         A[2] = cx(s2, zero); A[3] = cx(cs, zero);
         L.shape = SH_PAIR;
+        L.form = EF_ROTY;
         break;
       }
       case QSV_ROTATION_Z: {  // lambda_RotationZ + apply2, apply.hpp:117-128
@@ -234,6 +257,7 @@ inline qsv_status lower_gate(const qsv_gate& g, char op, int offset, int n,
         A[2] = cx(zero, zero); A[3] = l2;
         L.shape = SH_PAIR;
         L.diag = 1;
+        L.form = EF_DIAG;
         break;
       }
       case QSV_PHASE: {  // lambda_Phase, apply.hpp:132-140
@@ -295,6 +319,7 @@ inline qsv_status lower_gate(const qsv_gate& g, char op, int offset, int n,
         A[0] = cx(zero, zero); A[1] = cx(one, zero);
         A[2] = cx(one, zero);  A[3] = cx(zero, zero);
         L.shape = SH_CPAIR;
+        L.form = EF_SWAP;
         break;
       case QSV_CY: {  // CY.cpp:8-18: lambda_PauliY + apply4(ctrl)
         C<R> l1 = cx(zero, -one), l2 = cx(zero, one);
@@ -302,12 +327,14 @@ inline qsv_status lower_gate(const qsv_gate& g, char op, int offset, int n,
         A[0] = cx(zero, zero); A[1] = l1;
         A[2] = l2;             A[3] = cx(zero, zero);
         L.shape = SH_CPAIR;
+        L.form = EF_SWAP_MUL;
         break;
       }
       case QSV_CZ:  // CZ.cpp:8-18: lambda_PauliZ + apply4b
         A[0] = cx(-one, zero);
         count = 1;
         L.shape = SH_CHALF;
+        L.form = EF_NEG;
         break;
       case QSV_CPHASE: {  // CPhase.cpp:8-19: lambda_Phase + apply4b
         C<R> l = cx(cs, sn);
@@ -338,6 +365,7 @@ inline qsv_status lower_gate(const qsv_gate& g, char op, int offset, int n,
         A[2] = cx(zero, zero); A[3] = l2;
         L.shape = SH_CPAIR;
         L.diag = 1;
+        L.form = EF_DIAG;
         break;
       }
       case QSV_CONTROLLED1: {  // QControlledGate2.cpp:8-20

@@ -3,8 +3,9 @@
 
 Single-gate cases: every gate class x every op x qubit placements
 (n = 3: all placements; n = 6: low/high/mixed strides) x control states,
-on two inputs: x = 1..2^n (the input pattern of the reference's own gate
-tests, e.g. test/qgates/RotationX.cpp:288-300) and a seeded random vector.
+on three inputs: x = 1..2^n (the input pattern of the reference's own gate
+tests, e.g. test/qgates/RotationX.cpp:288-300), a seeded random vector and
+a vector of signed zeros and small exact values (special_input).
 Circuit cases: QFT (examples/qft.cpp:21-35), brick circuits and random
 mixed circuits, applied with all three ops and qubit offsets.
 """
@@ -49,6 +50,26 @@ def _two_qubit_gates(a, b, rng, real):
     return gs
 
 
+def same_bits(a, b) -> bool:
+    """Bitwise equality of two arrays: same dtype, shape and bytes (so -0 and
+    +0 differ, where np.array_equal calls them equal)."""
+    a, b = np.ascontiguousarray(a), np.ascontiguousarray(b)
+    return a.dtype == b.dtype and a.shape == b.shape and a.tobytes() == b.tobytes()
+
+
+def special_input(n, dtype, seed=0):
+    """Components drawn from {+0, -0, 1, -1, 1/2, -1/2, 2}: exact
+    cancellations and signed zeros, where a gate's arithmetic form (a swap,
+    a real scaling, a negation, a general complex product) shows in the sign
+    of zero results."""
+    vals = np.array([0.0, -0.0, 1.0, -1.0, 0.5, -0.5, 2.0])
+    x = np.zeros(1 << n, dtype=dtype)
+    comp = x.view(np.float32 if np.dtype(dtype) in (np.dtype(np.complex64),
+                                                    np.dtype(np.float32)) else np.float64)
+    comp[:] = np.random.default_rng(1000 + 7 * n + seed).choice(vals, size=comp.size)
+    return x
+
+
 def _inputs(n, dtype, rng):
     N = 1 << n
     iota = np.arange(1, N + 1).astype(dtype)
@@ -56,7 +77,7 @@ def _inputs(n, dtype, rng):
         rnd = (rng.normal(size=N) + 1j * rng.normal(size=N)).astype(dtype)
     else:
         rnd = rng.normal(size=N).astype(dtype)
-    return [iota, rnd]
+    return [iota, rnd, special_input(n, dtype)]
 
 
 def gate_cases(dtype):

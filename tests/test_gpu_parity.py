@@ -2,7 +2,8 @@
 reference's own outputs (golden fixtures), the CPU oracle, and each other.
 
 Tolerances:
-* reference-exact path (qsv_apply): bitwise equal (np.array_equal);
+* reference-exact path (qsv_apply): bitwise equal (same_bits: every byte,
+  signed zeros included);
 * fused path (qsv_apply_fused): max-abs 1e-12 for complex128/float64 and
   2e-5 for complex64/float32 on normalised states (the required bound for
   the 30-qubit brick is 1e-12 / 1e-5).
@@ -11,7 +12,7 @@ import numpy as np
 import pytest
 
 import oracle
-from cases import DTYPES, circuit_cases, gate_cases
+from cases import DTYPES, circuit_cases, gate_cases, same_bits
 from make_golden import HERE
 from qclab_b200 import QsvError, StateVector, launch_count
 from qclab_b200 import _lib as L
@@ -63,7 +64,7 @@ def test_every_gate_bitexact_vs_reference(states, dtype):
         y = run_gpu(states, n, dtype, recs, op, off, x)
         ref = gold[pos:pos + x.size]
         pos += x.size
-        assert np.array_equal(y, ref), (name, n, recs[0]["kind"], op, np.max(np.abs(y - ref)))
+        assert same_bits(y, ref), (name, n, recs[0]["kind"], op, np.max(np.abs(y - ref)))
     assert pos == gold.size
     assert launch_count() > before  # the CUDA kernels ran
 
@@ -73,7 +74,7 @@ def test_circuits_bitexact_vs_reference(states, dtype):
     name = np.dtype(dtype).name
     for cname, n, recs, op, off, x in circuit_cases(dtype):
         y = run_gpu(states, n, dtype, recs, op, off, x)
-        assert np.array_equal(y, GOLD[f"circ_{name}_{cname}"]), cname
+        assert same_bits(y, GOLD[f"circ_{name}_{cname}"]), cname
 
 
 @pytest.mark.parametrize("dtype", DTYPES, ids=lambda d: np.dtype(d).name)
@@ -114,7 +115,7 @@ def test_random_mixed_large(states, dtype, n):
     for op in "NC":
         ref = oracle.apply(x.copy(), recs, op)
         y = run_gpu(states, n, dtype, recs, op, 0, x)
-        assert np.array_equal(y, ref)
+        assert same_bits(y, ref)
         for opts in (None, L.FuseOpts(engine=1), L.FuseOpts(engine=2), L.FuseOpts(engine=3),
                      L.FuseOpts(engine=4), L.FuseOpts(engine=5), L.FuseOpts(engine=5, reg_bits=4)):
             yf = run_gpu(states, n, dtype, recs, op, 0, x, fused=True, opts=opts)
@@ -236,7 +237,7 @@ def test_qft20_config(states):
     x = np.zeros(1 << n, dtype=np.complex128)
     x[W.basis_index(n, seed=2024)] = 1
     ref = oracle.apply(x.copy(), recs)
-    assert np.array_equal(run_gpu(states, n, np.complex128, recs, "N", 0, x), ref)
+    assert same_bits(run_gpu(states, n, np.complex128, recs, "N", 0, x), ref)
     yf = run_gpu(states, n, np.complex128, recs, "N", 0, x, fused=True)
     assert np.max(np.abs(yf - ref)) <= 1e-12
 
@@ -260,7 +261,7 @@ def test_brick24_fused_vs_unfused(states):
     x[0] = 1
     ref = oracle.apply(x.copy(), recs)
     y = run_gpu(states, n, np.complex128, recs, "N", 0, x)
-    assert np.array_equal(y, ref)
+    assert same_bits(y, ref)
     yf = run_gpu(states, n, np.complex128, recs, "N", 0, x, fused=True)
     assert np.max(np.abs(yf - ref)) <= 1e-12
     assert abs(np.vdot(yf, yf).real - 1.0) < 1e-12
@@ -300,7 +301,7 @@ def test_circuit_offset_and_nesting(cuda):
             got = x.copy()
             circ.apply(op, 6, got, off)
             recs = circ.gate_records(np.complex128, offset=off)
-            assert np.array_equal(got, oracle.ref_apply(x, recs, op))
+            assert same_bits(got, oracle.ref_apply(x, recs, op))
 
 
 def test_wrap_caller_owned_device_memory(cuda):
@@ -320,7 +321,7 @@ def test_wrap_caller_owned_device_memory(cuda):
         circ.apply(op, n, sv)
         sv.synchronize()
         want = oracle.apply(x.copy(), circ.gate_records(np.complex128), op)
-        assert np.array_equal(t.cpu().numpy(), want), op
+        assert same_bits(t.cpu().numpy(), want), op
         sv.close()
     t = torch.from_numpy(x.copy()).to("cuda")
     sv = StateVector.wrap(t.data_ptr(), n, np.complex128)

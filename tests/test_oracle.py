@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle
-from cases import DTYPES, circuit_cases, gate_cases
+from cases import DTYPES, circuit_cases, gate_cases, same_bits
 from make_golden import HERE, case_digest
 from qclab_b200 import MatrixGate2, QCircuit
 from qclab_b200 import workloads as W
@@ -33,7 +33,7 @@ def test_oracle_bitexact_on_gate_fixtures(dtype):
     assert len(outs) == int(GOLD[f"gates_{name}_count"])
     assert hashlib.sha256("".join(digests).encode()).hexdigest() == str(GOLD[f"gates_{name}_digest"])
     got = np.concatenate(outs)
-    assert np.array_equal(got, GOLD[f"gates_{name}"])
+    assert same_bits(got, GOLD[f"gates_{name}"])
 
 
 @pytest.mark.parametrize("dtype", DTYPES, ids=lambda d: np.dtype(d).name)
@@ -42,7 +42,7 @@ def test_oracle_bitexact_on_circuit_fixtures(dtype):
     for cname, n, recs, op, off, x in circuit_cases(dtype):
         assert str(GOLD[f"circ_{name}_{cname}_digest"]) == case_digest(recs, op, off, x)
         y = oracle.apply(x.copy(), recs, op, off)
-        assert np.array_equal(y, GOLD[f"circ_{name}_{cname}"]), cname
+        assert same_bits(y, GOLD[f"circ_{name}_{cname}"]), cname
 
 
 @pytest.mark.skipif(not oracle.ref_available(), reason="reference not built here")
@@ -55,8 +55,8 @@ def test_oracle_bitexact_vs_reference_random(dtype):
             c = W.random_mixed(n - 1, 80, seed=seed, real=real)
             recs = c.gate_records(dtype)
             x = (rng.normal(size=1 << n) + (0 if real else 1j * rng.normal(size=1 << n))).astype(dtype)
-            assert np.array_equal(oracle.apply(x.copy(), recs, op, 1),
-                                  oracle.ref_apply(x.copy(), recs, op, 1))
+            assert same_bits(oracle.apply(x.copy(), recs, op, 1),
+                             oracle.ref_apply(x.copy(), recs, op, 1))
 
 
 def test_matrix_gate2_is_kron_basis():
