@@ -123,32 +123,20 @@ k_expect(const V* __restrict__ st, TileArgs ta, const DTerm* __restrict__ terms,
     tile[e] = st[tile_global(ta, ta.runoff, base, e)];
   stage_terms(ts, terms, nterms, base);
   __syncthreads();
-  // sum_t w_t sum_e conj(x_e) (-1)^popc(e & zy_t) x_{e ^ f_t}, over four
-  // independent accumulators (term t into acc[t % 4]) so consecutive terms'
-  // FMAs do not wait on each other
-  double2 acc[4] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0),
-                    make_double2(0.0, 0.0)};
-  auto term = [&](double2& a, const STerm& T, const double2 x, uint32_t e) {
-    const double2 y = to_d2(tile[e ^ T.flip_local]);
-    const double re = fma(x.x, y.x, x.y * y.y), im = fma(x.x, y.y, -x.y * y.x);
-    const double sg = (__popc(e & T.zy_local) & 1) ? -1.0 : 1.0;
-    a.x = fma(sg * T.wr, re, fma(-sg * T.wi, im, a.x));
-    a.y = fma(sg * T.wr, im, fma(sg * T.wi, re, a.y));
-  };
+  // sum_t w_t sum_e conj(x_e) (-1)^popc(e & zy_t) x_{e ^ f_t}
+  double2 acc = make_double2(0.0, 0.0);
   for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) {
     const double2 x = to_d2(tile[e]);
-    int t = 0;
-    for (; t + 4 <= nterms; t += 4) {
-      term(acc[0], ts[t], x, e);
-      term(acc[1], ts[t + 1], x, e);
-      term(acc[2], ts[t + 2], x, e);
-      term(acc[3], ts[t + 3], x, e);
+    for (int t = 0; t < nterms; ++t) {
+      const STerm T = ts[t];
+      const double2 y = to_d2(tile[e ^ T.flip_local]);
+      const double re = fma(x.x, y.x, x.y * y.y), im = fma(x.x, y.y, -x.y * y.x);
+      const double sg = (__popc(e & T.zy_local) & 1) ? -1.0 : 1.0;
+      acc.x = fma(sg * T.wr, re, fma(-sg * T.wi, im, acc.x));
+      acc.y = fma(sg * T.wr, im, fma(sg * T.wi, re, acc.y));
     }
-    for (; t < nterms; ++t) term(acc[0], ts[t], x, e);
   }
-  const double2 sum = make_double2((acc[0].x + acc[1].x) + (acc[2].x + acc[3].x),
-                                   (acc[0].y + acc[1].y) + (acc[2].y + acc[3].y));
-  const double2 r = block_sum(sum, red);
+  const double2 r = block_sum(acc, red);
   if (threadIdx.x == 0) partial[blockIdx.x] = r;
 }
 
@@ -166,24 +154,17 @@ k_observable(const V* __restrict__ src, V* __restrict__ dst, TileArgs ta,
     tile[e] = src[tile_global(ta, ta.runoff, base, e)];
   stage_terms(ts, terms, nterms, base);
   __syncthreads();
-  auto term = [&](double2& a, const STerm& T, uint32_t e) {
-    const double2 y = to_d2(tile[e ^ T.flip_local]);
-    const double sg = (__popc(e & T.zy_local) & 1) ? -1.0 : 1.0;
-    a.x = fma(sg * T.wr, y.x, fma(-sg * T.wi, y.y, a.x));
-    a.y = fma(sg * T.wr, y.y, fma(sg * T.wi, y.x, a.y));
-  };
   for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) {
     const uint64_t g = tile_global(ta, ta.runoff, base, e);
-    // two independent accumulators (term t into acc[t % 2])
-    double2 acc[2] = {accumulate ? to_d2(dst[g]) : make_double2(0.0, 0.0),
-                      make_double2(0.0, 0.0)};
-    int t = 0;
-    for (; t + 2 <= nterms; t += 2) {
-      term(acc[0], ts[t], e);
-      term(acc[1], ts[t + 1], e);
+    double2 acc = accumulate ? to_d2(dst[g]) : make_double2(0.0, 0.0);
+    for (int t = 0; t < nterms; ++t) {
+      const STerm T = ts[t];
+      const double2 y = to_d2(tile[e ^ T.flip_local]);
+      const double sg = (__popc(e & T.zy_local) & 1) ? -1.0 : 1.0;
+      acc.x = fma(sg * T.wr, y.x, fma(-sg * T.wi, y.y, acc.x));
+      acc.y = fma(sg * T.wr, y.y, fma(sg * T.wi, y.x, acc.y));
     }
-    if (t < nterms) term(acc[0], ts[t], e);
-    dst[g] = from_d2<V>(make_double2(acc[0].x + acc[1].x, acc[0].y + acc[1].y));
+    dst[g] = from_d2<V>(acc);
   }
 }
 

@@ -204,7 +204,9 @@ def _kernels(a) -> dict:
         reds = [("k_norm2 (norm)", lambda: st.norm2(), s16),
                 ("k_inner (inner product)", lambda: st.inner(other), 2 * s16),
                 ("k_compare (state comparison)", lambda: st.compare(other), 2 * s16),
-                ("k_expect* (Ising H, tiled groups)", lambda: st.expectation(H), None)]
+                ("k_expect* (Ising H, tiled groups)", lambda: st.expectation(H), None),
+                ("k_observable* (Ising H psi, tiled groups)", lambda: other.apply_observable(st, H),
+                 None)]
         for name, fn, nbytes in reds:
             ms = best(fn)
             out["kernels"][name] = {"ms": round(ms, 4),
