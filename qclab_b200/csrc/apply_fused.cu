@@ -554,6 +554,12 @@ __global__ void __launch_bounds__(256, 2)
                       a.coefs, a.ncoef, &passes, &ops, &coefs);
   if (a.tma.use) {
     if (!tma::tile_wait(&tile_bar, a.wait_error, tma::kTileWaitLimit)) return;
+    // the passes' address tables are for the cp.async layout (fewer bank
+    // conflicts in the MMA operand loads than the TMA swizzle gives)
+    if (a.tma.relayout) {
+      tma::relayout_rows(t0, (size * sizeof(V)) >> 7, a.tma.swz);
+      __syncthreads();
+    }
   } else {
     load_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
     __syncthreads();
@@ -630,9 +636,10 @@ __global__ void __launch_bounds__(256, 2)
     }
     __syncthreads();
   }
-  if (a.tma.use)
+  if (a.tma.use) {
+    if (a.tma.relayout) tma::relayout_rows(t0, (size * sizeof(V)) >> 7, a.tma.swz);  // back
     tma::tile_store<1>(a.tma, &tm0, &tm0, t0, nullptr, base);
-  else
+  } else
     store_tile<V, 1>(v0, nullptr, t0, nullptr, a.ta, base, a.vec16);
 }
 
@@ -1162,7 +1169,8 @@ qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool v
   for (size_t si = 0; si < plan.stages.size(); ++si) {
     geos[si] = TmaGeo{};
     const PackedStage& ps = plan.stages[si];
-    if (want_tma) tma_stage_map(ps.bits, ps.m, n, sizeof(V), x.v0, &maps[si], &geos[si]);
+    if (want_tma && tma_stage_map(ps.bits, ps.m, n, sizeof(V), x.v0, &maps[si], &geos[si]))
+      geos[si].relayout = 1;
   }
   for (size_t si = 0; si < plan.stages.size(); ++si) {
     const PackedStage& ps = plan.stages[si];
@@ -1173,8 +1181,8 @@ qsv_status execute_dmma(const ExecArgs& x, int m, int low, int max_gates, bool v
         return QSV_ERROR_NOT_SUPPORTED;
       if (tcg)
         tc_tables(&P, ps.m);
-      else
-        dmma_tables(&P, R, ps.m, Units<V>::per, geos[si].use ? geos[si].swz : -1);
+      else  // k_dmma3 converts TMA-staged tiles to the cp.async layout (relayout_rows)
+        dmma_tables(&P, R, ps.m, Units<V>::per, -1);
     }
   }
   unsigned* wait_error = sweep_wait_flag();

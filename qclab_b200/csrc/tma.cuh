@@ -47,6 +47,8 @@ struct TmaGeo {
   uint32_t box_bytes;  // bytes per copy and vector
   int wshift;          // log2(words per amplitude)
   int swz;             // B: log2(innermost box bytes / 16), the swizzle's XOR width
+  int relayout;        // 1: the kernel converts the tile to the cp.async layout after
+                       // the load and back before the store (relayout_rows)
   int8_t dstart[5];    // first word bit of each dimension's span
   int8_t dbits[5];     // width of each dimension's span (0: padding dimension)
   int8_t it[kTmaMaxIter];  // word bits of the iterated tile bits, ascending
@@ -181,6 +183,31 @@ __device__ __forceinline__ void tile_store(const TmaGeo& g, const CUtensorMap* m
 }
 
 constexpr int kTileWaitLimit = 2000;  // suspended polls (up to 1 ms each) for a tile load
+
+// Moves a tile between the TMA layout (unit u at u ^ ((u >> 3) & (2^B - 1)))
+// and the four-level XOR layout of the cp.async path (unit u at
+// u ^ ((u>>3 ^ u>>6 ^ u>>9 ^ u>>12) & 7), stage_exec.cuh phys): both keep
+// each 128-byte row in place and permute its eight 16-byte units by an XOR
+// that depends on the row r alone, so one layout becomes the other by
+// XOR-ing each row's unit index with
+//   d(r) = (r & (2^B - 1)) ^ ((r ^ r>>3 ^ r>>6 ^ r>>9) & 7)
+// -- an involution, the same call converts either way.  A warp takes four
+// whole rows at a time (lane = row * 8 + unit), reads them, then writes
+// them back permuted.  The caller synchronises the block around it.
+__device__ __forceinline__ void relayout_rows(void* tile, uint32_t rows, int B) {
+  float4* t = static_cast<float4*>(tile);
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const uint32_t mask = (1u << B) - 1u;
+  for (uint32_t r0 = warp * 4; r0 < rows; r0 += nwarps * 4) {
+    const uint32_t r = r0 + (lane >> 3), c = lane & 7u;
+    const bool ok = r < rows;
+    const uint32_t d = ((r & mask) ^ ((r ^ (r >> 3) ^ (r >> 6) ^ (r >> 9)) & 7u));
+    float4 v;
+    if (ok && d) v = t[r * 8 + c];
+    __syncwarp();
+    if (ok && d) t[r * 8 + (c ^ d)] = v;
+  }
+}
 
 // Dynamic shared memory from the next 1024-byte boundary (the launch
 // reserves 1024 bytes more than it uses).
