@@ -108,11 +108,26 @@ __device__ __forceinline__ double sgn_of(uint64_t x) {
   return (__popcll(x) & 1) ? -1.0 : 1.0;
 }
 
-// sum_t w_t sum_{j in tile} conj(psi_j) (-1)^{pop((j^f)&zy)} psi_{j^f}
+// Signed weight sum of a group's first ndiag terms (those without flip bits,
+// Z-strings): S(e) = sum_t w_t (-1)^popc(e & zy_t), so that they contribute
+// S(e) |x_e|^2 (expectation) or S(e) x_e (observable) with one product.
+__device__ __forceinline__ double2 diag_weight(const STerm* ts, int ndiag, uint32_t e) {
+  double sr = 0.0, si = 0.0;
+  for (int t = 0; t < ndiag; ++t) {
+    const STerm& T = ts[t];
+    const bool odd = __popc(e & T.zy_local) & 1;
+    sr += odd ? -T.wr : T.wr;
+    si += odd ? -T.wi : T.wi;
+  }
+  return make_double2(sr, si);
+}
+
+// sum_t w_t sum_{j in tile} conj(psi_j) (-1)^{pop((j^f)&zy)} psi_{j^f}; the
+// group's first ndiag terms have no flip bits
 template <typename V>
 __global__ void __launch_bounds__(kRedThreads)
 k_expect(const V* __restrict__ st, TileArgs ta, const DTerm* __restrict__ terms, int nterms,
-         double2* __restrict__ partial) {
+         int ndiag, double2* __restrict__ partial) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* tile = reinterpret_cast<V*>(smem_raw);
   const uint32_t size = 1u << ta.m;
@@ -127,7 +142,13 @@ k_expect(const V* __restrict__ st, TileArgs ta, const DTerm* __restrict__ terms,
   double2 acc = make_double2(0.0, 0.0);
   for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) {
     const double2 x = to_d2(tile[e]);
-    for (int t = 0; t < nterms; ++t) {
+    if (ndiag > 0) {
+      const double2 S = diag_weight(ts, ndiag, e);
+      const double p = fma(x.x, x.x, x.y * x.y);
+      acc.x = fma(S.x, p, acc.x);
+      acc.y = fma(S.y, p, acc.y);
+    }
+    for (int t = ndiag; t < nterms; ++t) {
       const STerm T = ts[t];
       const double2 y = to_d2(tile[e ^ T.flip_local]);
       const double re = fma(x.x, y.x, x.y * y.y), im = fma(x.x, y.y, -x.y * y.x);
@@ -140,11 +161,12 @@ k_expect(const V* __restrict__ st, TileArgs ta, const DTerm* __restrict__ terms,
   if (threadIdx.x == 0) partial[blockIdx.x] = r;
 }
 
-// dst (+)= sum_t w_t P_t src over one tile group
+// dst (+)= sum_t w_t P_t src over one tile group (first ndiag terms without
+// flip bits)
 template <typename V>
 __global__ void __launch_bounds__(kRedThreads)
 k_observable(const V* __restrict__ src, V* __restrict__ dst, TileArgs ta,
-             const DTerm* __restrict__ terms, int nterms, int accumulate) {
+             const DTerm* __restrict__ terms, int nterms, int ndiag, int accumulate) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V* tile = reinterpret_cast<V*>(smem_raw);
   const uint32_t size = 1u << ta.m;
@@ -157,7 +179,13 @@ k_observable(const V* __restrict__ src, V* __restrict__ dst, TileArgs ta,
   for (uint32_t e = threadIdx.x; e < size; e += blockDim.x) {
     const uint64_t g = tile_global(ta, ta.runoff, base, e);
     double2 acc = accumulate ? to_d2(dst[g]) : make_double2(0.0, 0.0);
-    for (int t = 0; t < nterms; ++t) {
+    if (ndiag > 0) {
+      const double2 S = diag_weight(ts, ndiag, e);
+      const double2 x = to_d2(tile[e]);
+      acc.x = fma(S.x, x.x, fma(-S.y, x.y, acc.x));
+      acc.y = fma(S.x, x.y, fma(S.y, x.x, acc.y));
+    }
+    for (int t = ndiag; t < nterms; ++t) {
       const STerm T = ts[t];
       const double2 y = to_d2(tile[e ^ T.flip_local]);
       const double sg = (__popc(e & T.zy_local) & 1) ? -1.0 : 1.0;
@@ -314,12 +342,20 @@ qsv_status run_tiled(qsv_state_s* s, const V* src, V* dst, const std::vector<HTe
   std::vector<DTerm> dt;
   std::vector<uint64_t> runoffs;
   std::vector<size_t> term0;
+  std::vector<int> ndiag;
   for (const Group& G : groups) {
     int local_of[64];
     for (int j = 0; j < 64; ++j) local_of[j] = -1;
     for (int j = 0; j < G.m; ++j) local_of[G.bits[j]] = j;
     term0.push_back(dt.size());
-    for (int ti : G.terms) {
+    // terms without flip bits first (their contributions share one product)
+    std::vector<int> order;
+    for (int ti : G.terms)
+      if (T[ti].flip == 0) order.push_back(ti);
+    ndiag.push_back((int)order.size());
+    for (int ti : G.terms)
+      if (T[ti].flip != 0) order.push_back(ti);
+    for (int ti : order) {
       const HTerm& h = T[ti];
       DTerm d{};
       for (int b = 0; b < n; ++b) {
@@ -379,11 +415,11 @@ qsv_status run_tiled(qsv_state_s* s, const V* src, V* dst, const std::vector<HTe
     const DTerm* terms = reinterpret_cast<const DTerm*>(dev + term_off) + term0[gi];
     const int nt = (int)groups[gi].terms.size();
     if (expect)
-      k_expect<V><<<(unsigned)ntiles, threads, smem, s->stream>>>(src, ta, terms, nt,
+      k_expect<V><<<(unsigned)ntiles, threads, smem, s->stream>>>(src, ta, terms, nt, ndiag[gi],
                                                                  partial + gi * ntiles);
     else
       k_observable<V><<<(unsigned)ntiles, threads, smem, s->stream>>>(src, dst, ta, terms, nt,
-                                                                      gi > 0 ? 1 : 0);
+                                                                      ndiag[gi], gi > 0 ? 1 : 0);
     count_launch();
     if (qsv_status st = cuda_status(cudaGetLastError(), "tiled reduction launch")) return st;
   }
