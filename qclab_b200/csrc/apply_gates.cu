@@ -245,9 +245,61 @@ __device__ __forceinline__ void op_scale(V (&x)[N], const V* __restrict__ c) {
 //   RDZ: conj(lam_j) (-1)^{bit p of j} psi_j      -> Im
 // in FP64, reduced over the warp into the term's shared-memory accumulator
 // (stage_exec.cuh: red_accumulate).
-template <int K, int P, typename V, int N>
+// G_RDG: any generator, masks read from c[1] (gate_plan.hpp KindR).  The
+// flip mask f selects one of 2^R compile-time variants (a switch), so the
+// partner registers x[j ^ F] stay compile-time indices.
+template <int F, typename V, int N>
+__device__ __forceinline__ void red_generic_f(const V (&x)[N], const V (&y)[N], uint32_t zy,
+                                              uint32_t pm, uint32_t pv, double& sr, double& si) {
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    if ((j & pm) != pv) continue;
+    const double2 a = to_d2(y[j]), b = to_d2(x[j ^ F]);
+    const double re = fma(a.x, b.x, a.y * b.y), im = fma(a.x, b.y, -a.y * b.x);
+    if (__popc((j ^ F) & zy) & 1) {
+      sr -= re;
+      si -= im;
+    } else {
+      sr += re;
+      si += im;
+    }
+  }
+}
+
+template <int F, typename V, int N>
+__device__ __forceinline__ void red_generic_sel(uint32_t f, const V (&x)[N], const V (&y)[N],
+                                                uint32_t zy, uint32_t pm, uint32_t pv, double& sr,
+                                                double& si) {
+  if constexpr (F < N) {
+    if (f == F)
+      red_generic_f<F>(x, y, zy, pm, pv, sr, si);
+    else
+      red_generic_sel<F + 1>(f, x, y, zy, pm, pv, sr, si);
+  }
+}
+
+template <typename V, int N>
+__device__ __forceinline__ void red_generic(const V (&x)[N], const V (&y)[N], const V* __restrict__ c,
+                                            double* racc, unsigned lanes) {
+  const double2 c0 = to_d2(c[0]), c1 = to_d2(c[1]);
+  const uint32_t pk = (uint32_t)c1.x;
+  const uint32_t f = pk & 31u, zy = (pk >> 5) & 31u, pm = (pk >> 10) & 31u, pv = (pk >> 15) & 31u;
+  double sr = 0.0, si = 0.0;
+  red_generic_sel<0>(f, x, y, zy, pm, pv, sr, si);
+  // Im(i^ny s)
+  const int ny = (int)c1.y & 3;
+  const double v = ny == 0 ? si : ny == 1 ? sr : ny == 2 ? -si : -sr;
+  fx::red_accumulate(c0.x * v, (int)c0.y, racc, lanes);
+}
+
+template <int K, int P, bool GEN, typename V, int N>
 __device__ __forceinline__ void red_op(const V (&x)[N], const V (&y)[N], const V* __restrict__ c,
                                        double* racc, unsigned lanes) {
+  if constexpr (K == G_RDG) {  // only in the kernels built for stages that hold one
+    if constexpr (GEN) red_generic(x, y, c, racc, lanes);
+    else __builtin_unreachable();
+    return;
+  }
   constexpr int M = 1 << P;
   double sr = 0.0, si = 0.0;
 #pragma unroll
@@ -271,8 +323,9 @@ __device__ __forceinline__ void red_op(const V (&x)[N], const V (&y)[N], const V
 // One op word (device_word in gate_plan.hpp): kind (bits 0-4), register
 // position index (bits 5-10), coefficient index (bits 11-31); a two-level
 // switch (gate_cases.inc).  With NV = 2 every op acts on psi (x) and
-// lambda (y) and gradient terms accumulate into racc.
-template <typename V, int R, int NV>
+// lambda (y) and gradient terms accumulate into racc.  GEN: the stage holds
+// G_RDG terms (a separate kernel, whose extra registers the others do not pay).
+template <typename V, int R, int NV, bool GEN>
 __device__ __forceinline__ void apply_word(V (&x)[1 << R], V (&y)[1 << R], uint32_t w,
                                            const V* __restrict__ cf, double* racc,
                                            unsigned lanes) {
@@ -286,7 +339,7 @@ __device__ __forceinline__ void apply_word(V (&x)[1 << R], V (&y)[1 << R], uint3
   } while (0)
 #define GXR(K, P)                                                   \
   do {                                                              \
-    if constexpr (NV == 2) red_op<K, P>(x, y, c, racc, lanes);      \
+    if constexpr (NV == 2) red_op<K, P, GEN>(x, y, c, racc, lanes); \
   } while (0)
   if constexpr (R == 3) {
     QSV_GX_NESTED_3
@@ -342,7 +395,7 @@ __device__ __forceinline__ uint32_t reg_off(uint32_t ptb, const uint32_t (&boff)
   return o;
 }
 
-template <typename V, int R, int NT, int MINB, int NV>
+template <typename V, int R, int NT, int MINB, int NV, bool GEN = false>
 __global__ void __launch_bounds__(NT, MINB)
     k_gates(V* __restrict__ v0, V* __restrict__ v1, GxArgs a,
             const __grid_constant__ CUtensorMap tm0, const __grid_constant__ CUtensorMap tm1) {
@@ -416,7 +469,8 @@ __global__ void __launch_bounds__(NT, MINB)
           if (NV == 2) y[j] = t1[o];
         }
       }
-      for (int o = 0; o < nops; ++o) apply_word<V, R, NV>(x, y, ops[op0 + o], coefs, racc, lanes);
+      for (int o = 0; o < nops; ++o)
+        apply_word<V, R, NV, GEN>(x, y, ops[op0 + o], coefs, racc, lanes);
       // the store recomputes the offsets: without this the compiler keeps
       // all 2^R of them live across the ops for reuse, which costs registers
       // the amplitudes need
@@ -467,16 +521,18 @@ __global__ void __launch_bounds__(NT, MINB)
 // register groups per pass.
 template <typename V> struct GxKernels;
 template <> struct GxKernels<double2> {
-  static void* get(int R, int ctas, int nv) {
-    if (nv == 2) return (void*)k_gates<double2, 3, 128, 3, 2>;
+  static void* get(int R, int ctas, int nv, bool gen = false) {
+    if (nv == 2)
+      return gen ? (void*)k_gates<double2, 3, 128, 3, 2, true> : (void*)k_gates<double2, 3, 128, 3, 2>;
     return ctas == 3 ? (void*)k_gates<double2, 4, 128, 3, 1>
                      : (void*)k_gates<double2, 4, 128, 2, 1>;
   }
   static int threads(int R, int nv) { (void)R; (void)nv; return 128; }
 };
 template <> struct GxKernels<float2> {
-  static void* get(int R, int ctas, int nv) {
-    if (nv == 2) return (void*)k_gates<float2, 4, 128, 3, 2>;
+  static void* get(int R, int ctas, int nv, bool gen = false) {
+    if (nv == 2)
+      return gen ? (void*)k_gates<float2, 4, 128, 3, 2, true> : (void*)k_gates<float2, 4, 128, 3, 2>;
     if (R == 5) return (void*)k_gates<float2, 5, 128, 2, 1>;
     return ctas == 2 ? (void*)k_gates<float2, 4, 256, 2, 1> : (void*)k_gates<float2, 4, 256, 3, 1>;
   }
@@ -601,11 +657,24 @@ qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool 
   if (qsv_status st = cuda_status(cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice,
                                                   s->stream), "gate plan upload"))
     return st;
-  void* kern = GxKernels<V>::get(R, x.opts ? x.opts->ctas_per_sm : 0, nv);
-  if (qsv_status st = cuda_status(cudaFuncSetAttribute(kern,
-                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       200 * 1024), "gate stage shared-memory attribute"))
-    return st;
+  // two-vector stages with generic gradient terms (G_RDG) run the kernel
+  // built with them
+  const int ctas = x.opts ? x.opts->ctas_per_sm : 0;
+  const uint32_t rdg = (uint32_t)code_red(R, G_RDG, 0);
+  std::vector<char> stage_gen(plan.stages.size(), 0);
+  for (size_t si = 0; si < plan.stages.size(); ++si) {
+    const GxStage& gs = plan.stages[si];
+    for (size_t o = gs.op0; o < gs.op0 + gs.nops; ++o)
+      if ((plan.ops[o] & ((1u << kCodeBits) - 1u)) == rdg) stage_gen[si] = 1;
+  }
+  for (bool gen : {false, true}) {
+    if (gen && nv != 2) break;
+    if (qsv_status st = cuda_status(cudaFuncSetAttribute(GxKernels<V>::get(R, ctas, nv, gen),
+                                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                         200 * 1024),
+                                    "gate stage shared-memory attribute"))
+      return st;
+  }
   const uint64_t ntiles = 1ull << (n - m);
   if (x.ntiles_out) *x.ntiles_out = ntiles;
   const unsigned threads =
@@ -643,6 +712,7 @@ qsv_status execute_gates(const ExecArgs& x, int m, int low, int max_gates, bool 
       return fail(QSV_ERROR_SIZE, "gate stage needs %zu bytes of shared memory", smem);
     a.smem_bytes = (uint32_t)smem;
     void* args[] = {&p0, &p1, &a, &maps[2 * si], &maps[2 * si + (nv == 2 ? 1 : 0)]};
+    void* kern = GxKernels<V>::get(R, ctas, nv, nv == 2 && stage_gen[si]);
     if (qsv_status st = cuda_status(cudaLaunchKernel(kern, dim3((unsigned)ntiles), dim3(threads),
                                                      args, smem, s->stream),
                                     "gate stage launch"))

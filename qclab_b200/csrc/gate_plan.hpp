@@ -54,8 +54,13 @@ enum Kind4 : int { G_SWAP, G_ISWAP, G_GEN4, G_N4 };
 // gradient terms of the two-vector (adjoint) sweeps at register position p:
 // Im <lam| X_p |psi>, Re <lam| Y_p |psi> (= Im(i <lam|Y_p|psi>)) and
 // Im <lam| Z_p |psi>, the derivatives of RotationX/Y/Z (lower.hpp:
-// generator_of, weight 1, no projector)
-enum KindR : int { G_RDX, G_RDY, G_RDZ, G_NR };
+// generator_of, weight 1, no projector); and G_RDG (position 0 only) for
+// every other generator -- a Pauli string with flip mask f, sign mask zy and
+// ny Y factors, a projector (pm, pv) and a weight w, all its bits in the pass:
+//   w Im(i^ny sum_{j: (j & pm) == pv} conj(lam_j) (-1)^popc((j^f) & zy) psi_{j^f})
+// with coefficients c[0] = (|kappa|^2 w, term index) and
+// c[1] = (f | zy << 5 | pm << 10 | pv << 15 as register masks, ny).
+enum KindR : int { G_RDX, G_RDY, G_RDZ, G_RDG, G_NR };
 
 // Dense case codes for R register bits (holes where p = q are never used).
 constexpr int code1(int R, int k, int p) { return k * R + p; }
@@ -406,6 +411,16 @@ inline void host_apply_op2(cplx* x, cplx* y, int R, uint32_t word, const cplx* c
   }
   const int r = code - code_red(R, 0, 0), k = r / R, p = r % R, mp = 1 << p;
   cplx s(0.0, 0.0);
+  if (k == G_RDG) {
+    const uint32_t pk = (uint32_t)c[1].real();
+    const int f = pk & 31, zy = (pk >> 5) & 31, pm = (pk >> 10) & 31, pv = (pk >> 15) & 31;
+    for (int j = 0; j < (1 << R); ++j)
+      if ((j & pm) == pv)
+        s += std::conj(y[j]) * ((__builtin_popcount((j ^ f) & zy) & 1) ? -1.0 : 1.0) * x[j ^ f];
+    static const cplx ipow[4] = {cplx(1, 0), cplx(0, 1), cplx(-1, 0), cplx(0, -1)};
+    red[(int)c[0].imag()] += c[0].real() * (ipow[(int)c[1].imag() & 3] * s).imag();
+    return;
+  }
   for (int j = 0; j < (1 << R); ++j) {
     const int f = (k == G_RDZ) ? j : (j ^ mp);
     double sg = 1.0;
@@ -477,17 +492,8 @@ inline bool pack_gate_plan(const std::vector<Lowered>& gates, int n, int m, int 
   // every tile needs a bit outside its contiguous low bits unless it holds
   // the whole state
   if (m < R || R > kMaxR || (low >= m && m < n)) return false;
-  for (const Lowered& L : gates) {
-    if (L.shape != SH_RED) continue;
-    if (!two_vector) return false;
-    // the generators this engine evaluates: one X, Y or Z factor, weight 1
-    const Generator& g = L.gen;
-    const uint64_t b = g.f | g.zy;
-    if (g.pm || g.w != 1 || __builtin_popcountll(b) != 1) return false;
-    const bool x = g.f == b && g.zy == 0 && g.ny == 0, y = g.f == b && g.zy == b && g.ny == 1,
-               z = g.f == 0 && g.zy == b && g.ny == 0;
-    if (!(x || y || z)) return false;
-  }
+  for (const Lowered& L : gates)
+    if (L.shape == SH_RED && !two_vector) return false;
   const std::vector<Stage> stages =
       plan_stages(gates, n, m, low, max_gates, two_vector ? kMaxStageRed : 0, plan_cap,
                   elem_bytes);
@@ -527,15 +533,33 @@ inline bool pack_gate_plan(const std::vector<Lowered>& gates, int n, int m, int 
       for (int oi : p.ops) {
         const Lowered& L = gates[stg.gates[oi]];
         if (L.shape == SH_RED) {
-          // coefficient: (|kappa|^2 so far, term index)
-          const uint64_t b = L.gen.f | L.gen.zy;
-          const int r0 = reg_of[local_of[__builtin_ctzll(b)]];
-          const int k = L.gen.zy == 0 ? G_RDX : (L.gen.f == 0 ? G_RDZ : G_RDY);
           if (gs.nred >= kMaxStageRed) return false;
+          const Generator& g = L.gen;
+          const uint64_t b = g.f | g.zy;
+          const bool one = !g.pm && g.w == 1 && __builtin_popcountll(b) == 1;
+          const bool x = one && g.f == b && g.zy == 0 && g.ny == 0;
+          const bool y = one && g.f == b && g.zy == b && g.ny == 1;
+          const bool z = one && g.f == 0 && g.zy == b && g.ny == 0;
           GxOp op;
-          op.code = code_red(R, k, r0);
-          op.ncoef = 1;
-          op.c[0] = cplx(std::norm(kappa), (double)gs.nred++);
+          if (x || y || z) {  // coefficient: (|kappa|^2 so far, term index)
+            const int r0 = reg_of[local_of[__builtin_ctzll(b)]];
+            op.code = code_red(R, x ? G_RDX : (z ? G_RDZ : G_RDY), r0);
+            op.ncoef = 1;
+            op.c[0] = cplx(std::norm(kappa), (double)gs.nred++);
+          } else {  // any other generator: its masks as register masks
+            auto regmask = [&](uint64_t gm) {
+              uint32_t r = 0;
+              for (int q = 0; q < n; ++q)
+                if ((gm >> q) & 1ull) r |= 1u << reg_of[local_of[q]];
+              return r;
+            };
+            const uint32_t pk = regmask(g.f) | regmask(g.zy) << 5 | regmask(g.pm) << 10 |
+                                regmask(g.pv) << 15;
+            op.code = code_red(R, G_RDG, 0);
+            op.ncoef = 2;
+            op.c[0] = cplx(std::norm(kappa) * g.w, (double)gs.nred++);
+            op.c[1] = cplx((double)pk, (double)(g.ny & 3));
+          }
           ops.push_back(op);
           out->red_slots.push_back(L.slot);
           continue;

@@ -16,7 +16,7 @@ KIND1 = ["G_H", "G_SHEAR", "G_SHEARO", "G_ISHEAR", "G_ISHEARO", "G_PHASE", "G_GE
          "G_X", "G_Z"]
 KIND2 = ["G_CX", "G_CGEN2", "G_CNEG", "G_CPH"]
 KIND4 = ["G_SWAP", "G_ISWAP", "G_GEN4"]
-KINDR = ["G_RDX", "G_RDY", "G_RDZ"]
+KINDR = ["G_RDX", "G_RDY", "G_RDZ", "G_RDG"]
 
 
 def nested(R: int) -> list[str]:
@@ -49,6 +49,9 @@ def nested(R: int) -> list[str]:
     out.append(f"case {k0}: GX1(op_scale); break;")
     k0 += 1
     for k, name in enumerate(KINDR):
+        if name == "G_RDG":  # any generator: masks in its coefficients, position 0
+            out.append(f"case {k0 + k}: GXR({name}, 0); break;")
+            continue
         out.append(f"case {k0 + k}: switch (sub) {{")
         for p in range(R):
             out.append(f"  case {p}: GXR({name}, {p}); break;")

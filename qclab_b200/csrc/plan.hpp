@@ -54,6 +54,7 @@ inline size_t plan_bytes_of(const Lowered& L, size_t elem_bytes) {
     case SH_PAIR: case SH_CPAIR: nc = 4; break;
     case SH_QUAD: nc = 16; break;
     case SH_HALF: case SH_CHALF: case SH_SWAP: nc = 1; break;
+    case SH_RED: nc = 2; break;
     default: break;
   }
   return 24 + 80 + size_t(nc) * elem_bytes;

@@ -127,3 +127,63 @@ def test_adjoint_gradient_terms(binary, tmp_path, R, m, low):
             continue
         ps = 0.5 * (energy(_shifted(recs, k, np.pi / 2)) - energy(_shifted(recs, k, -np.pi / 2)))
         assert abs(grad[p] - ps) < 1e-10, (p, grad[p], ps)
+
+
+@pytest.mark.parametrize("R,m,low", [(3, 8, 2), (4, 10, 3)])
+def test_adjoint_gradient_terms_any_generator(binary, tmp_path, R, m, low):
+    """Gradient terms of every trainable gate class (two-qubit rotations,
+    controlled rotations with either control state, Phase and CPhase) as
+    generic RDG ops, against central finite differences on the oracle."""
+    from qclab_b200 import gates as G
+    from qclab_b200.circuit import QCircuit
+    from qclab_b200.gradients import _shifted
+    from qclab_b200.observable import ising
+    n = 9
+    rng = np.random.default_rng(R * 100 + m)
+    ang = lambda: float(rng.uniform(0, 6.28))  # noqa: E731
+    c = QCircuit(n)
+    for layer in range(2):
+        for q in range(n):
+            c.push_back((G.RotationX, G.RotationY, G.RotationZ)[q % 3](q, ang()))
+        c.push_back(G.RotationXX(0, n - 1, ang()))
+        c.push_back(G.RotationYY(2, 5, ang()))
+        c.push_back(G.RotationZZ(1, 7, ang()))
+        c.push_back(G.CRotationX(3, 0, ang(), controlState=layer))
+        c.push_back(G.CRotationY(8, 2, ang(), controlState=1 - layer))
+        c.push_back(G.CRotationZ(4, 6, ang()))
+        c.push_back(G.CPhase(0, 4, ang()))
+        c.push_back(G.Phase(6, ang()))
+        for q in range(layer % 2, n - 1, 2):
+            c.push_back(G.CNOT(q, q + 1))
+    recs = c.gate_records(np.complex128, number_params=True)
+    terms = ising(n).matrix_free_terms()
+    psi = np.zeros(1 << n, dtype=np.complex128)
+    psi[0] = 1
+    oracle.apply(psi, recs)
+    lam = oracle.observable_apply(psi, terms)
+    rp, pp, lp, op_ = (tmp_path / f for f in ("r.bin", "p.bin", "l.bin", "o.bin"))
+    rp.write_bytes(recs.tobytes())
+    pp.write_bytes(psi.tobytes())
+    lp.write_bytes(lam.tobytes())
+    r = subprocess.run([str(binary), "adjoint", str(n), str(R), str(m), str(low), str(rp), str(pp),
+                        str(lp), str(op_)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    rows = np.frombuffer(op_.read_bytes(), dtype=np.float64)
+    params = [int(recs[k]["param"]) for k in range(len(recs) - 1, -1, -1) if recs[k]["param"] >= 0]
+    grad = np.zeros(int(recs["param"].max()) + 1)
+    for slot, p in enumerate(params):
+        grad[p] += rows[slot]
+
+    def energy(rr):
+        x = np.zeros(1 << n, dtype=np.complex128)
+        x[0] = 1
+        oracle.apply(x, rr)
+        return oracle.expectation(x, terms)
+
+    h = 1e-6
+    for k in range(len(recs)):
+        p = int(recs[k]["param"])
+        if p < 0:
+            continue
+        fd = (energy(_shifted(recs, k, h)) - energy(_shifted(recs, k, -h))) / (2 * h)
+        assert abs(grad[p] - fd) < 1e-7, (p, int(recs[k]["kind"]), grad[p], fd)
