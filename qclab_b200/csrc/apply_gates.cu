@@ -50,12 +50,17 @@ __device__ __forceinline__ V mk(T a, T b) { return V{a, b}; }
 // to op: written as plain C++, the switch's cases each produced new values
 // that the compiler then copied back at the loop join, several moves per
 // amplitude per op.
-__device__ __forceinline__ void ip_h(double& a, double& b) {  // (a + b, a - b)
-  asm("{\n .reg .f64 t;\n add.rn.f64 t, %0, %1;\n sub.rn.f64 %1, %0, %1;\n mov.f64 %0, t;\n}"
+// (a + b, a - b) in two instructions and no move: b' = a - b, then
+// a' = 2a - b' (= a + b up to the rounding of b', one more rounding error of
+// the size of the other's)
+__device__ __forceinline__ void ip_h(double& a, double& b) {
+  asm("{\n .reg .f64 t;\n sub.rn.f64 %1, %0, %1;\n neg.f64 t, %1;\n"
+      " fma.rn.f64 %0, %0, 0d4000000000000000, t;\n}"
       : "+d"(a), "+d"(b));
 }
 __device__ __forceinline__ void ip_h(float& a, float& b) {
-  asm("{\n .reg .f32 t;\n add.rn.f32 t, %0, %1;\n sub.rn.f32 %1, %0, %1;\n mov.f32 %0, t;\n}"
+  asm("{\n .reg .f32 t;\n sub.rn.f32 %1, %0, %1;\n neg.f32 t, %1;\n"
+      " fma.rn.f32 %0, %0, 0f40000000, t;\n}"
       : "+f"(a), "+f"(b));
 }
 // (a + p b, q a + b)
@@ -122,17 +127,16 @@ __device__ __forceinline__ void ip_negv(V& a) {
 
 // ---- ops (positions compile-time; x: the thread's N = 2^R registers) --------
 template <int K, int P, typename V, int N>
-__device__ __forceinline__ void op1(V (&x)[N], const V* __restrict__ c) {
+__device__ __forceinline__ void op1(V (&x)[N], const V* __restrict__ c, const V cw) {
   using T = typename RealOf<V>::T;
   constexpr int M = 1 << P;
   T ca = T(0), cb = T(0);
   V c0{};
   if constexpr (K == G_SHEAR || K == G_SHEARO || K == G_ISHEAR || K == G_ISHEARO) {
-    const V cc = c[0];
-    ca = cc.x;
-    cb = cc.y;
+    ca = cw.x;
+    cb = cw.y;
   } else if constexpr (K == G_PHASE) {
-    c0 = c[0];
+    c0 = cw;
   }
 #pragma unroll
   for (int j = 0; j < N; ++j) {
@@ -178,10 +182,10 @@ __device__ __forceinline__ void op1(V (&x)[N], const V* __restrict__ c) {
 }
 
 template <int K, int Pt, int Pc, int CV, typename V, int N>
-__device__ __forceinline__ void op2(V (&x)[N], const V* __restrict__ c) {
+__device__ __forceinline__ void op2(V (&x)[N], const V* __restrict__ c, const V cw) {
   constexpr int MT = 1 << Pt, MC = 1 << Pc;
   V c0{};
-  if constexpr (K == G_CPH) c0 = c[0];
+  if constexpr (K == G_CPH) c0 = cw;
 #pragma unroll
   for (int j = 0; j < N; ++j) {
     if ((j & MT) || (((j & MC) ? 1 : 0) != CV)) continue;
@@ -203,10 +207,10 @@ __device__ __forceinline__ void op2(V (&x)[N], const V* __restrict__ c) {
 }
 
 template <int K, int P0, int P1, typename V, int N>
-__device__ __forceinline__ void op4(V (&x)[N], const V* __restrict__ c) {
+__device__ __forceinline__ void op4(V (&x)[N], const V* __restrict__ c, const V cw) {
   constexpr int M0 = 1 << P0, M1 = 1 << P1;
   V z{};
-  if constexpr (K == G_ISWAP) z = c[0];
+  if constexpr (K == G_ISWAP) z = cw;
 #pragma unroll
   for (int j = 0; j < N; ++j) {
     if ((j & M0) || (j & M1)) continue;
@@ -232,8 +236,9 @@ __device__ __forceinline__ void op4(V (&x)[N], const V* __restrict__ c) {
 }
 
 template <typename V, int N>
-__device__ __forceinline__ void op_scale(V (&x)[N], const V* __restrict__ c) {
-  const V z = c[0];
+__device__ __forceinline__ void op_scale(V (&x)[N], const V* __restrict__ c, const V cw) {
+  (void)c;
+  const V z = cw;
 #pragma unroll
   for (int j = 0; j < N; ++j) ip_cmulv(x[j], z);
 }
@@ -294,7 +299,7 @@ __device__ __forceinline__ void red_generic(const V (&x)[N], const V (&y)[N], co
 
 template <int K, int P, bool GEN, typename V, int N>
 __device__ __forceinline__ void red_op(const V (&x)[N], const V (&y)[N], const V* __restrict__ c,
-                                       double* racc, unsigned lanes) {
+                                       const V cw, double* racc, unsigned lanes) {
   if constexpr (K == G_RDG) {  // only in the kernels built for stages that hold one
     if constexpr (GEN) red_generic(x, y, c, racc, lanes);
     else __builtin_unreachable();
@@ -316,30 +321,32 @@ __device__ __forceinline__ void red_op(const V (&x)[N], const V (&y)[N], const V
       si += im;
     }
   }
-  const double2 cc = to_d2(c[0]);
+  const double2 cc = to_d2(cw);
   fx::red_accumulate(cc.x * ((K == G_RDY) ? sr : si), (int)cc.y, racc, lanes);
 }
 
 // One op word (device_word in gate_plan.hpp): kind (bits 0-4), register
 // position index (bits 5-10), coefficient index (bits 11-31); a two-level
-// switch (gate_cases.inc).  With NV = 2 every op acts on psi (x) and
+// switch (gate_cases.inc).  cw = the op's first coefficient, loaded by the
+// caller before the switch (every stage's coefficient table has at least one
+// entry, and ops without coefficients index entry 0).  With NV = 2 every op acts on psi (x) and
 // lambda (y) and gradient terms accumulate into racc.  GEN: the stage holds
 // G_RDG terms (a separate kernel, whose extra registers the others do not pay).
 template <typename V, int R, int NV, bool GEN>
 __device__ __forceinline__ void apply_word(V (&x)[1 << R], V (&y)[1 << R], uint32_t w,
-                                           const V* __restrict__ cf, double* racc,
+                                           const V cw, const V* __restrict__ cf, double* racc,
                                            unsigned lanes) {
   const V* __restrict__ c = cf + (w >> kWordCoefShift);
   const uint32_t kind = w & ((1u << kKindBits) - 1u);
   const uint32_t sub = (w >> kKindBits) & ((1u << kSubBits) - 1u);
 #define GX1(f)                      \
   do {                              \
-    f(x, c);                        \
-    if constexpr (NV == 2) f(y, c); \
+    f(x, c, cw);                        \
+    if constexpr (NV == 2) f(y, c, cw); \
   } while (0)
 #define GXR(K, P)                                                   \
   do {                                                              \
-    if constexpr (NV == 2) red_op<K, P, GEN>(x, y, c, racc, lanes); \
+    if constexpr (NV == 2) red_op<K, P, GEN>(x, y, c, cw, racc, lanes); \
   } while (0)
   if constexpr (R == 3) {
     QSV_GX_NESTED_3
@@ -469,8 +476,10 @@ __global__ void __launch_bounds__(NT, MINB)
           if (NV == 2) y[j] = t1[o];
         }
       }
-      for (int o = 0; o < nops; ++o)
-        apply_word<V, R, NV, GEN>(x, y, ops[op0 + o], coefs, racc, lanes);
+      for (int o = 0; o < nops; ++o) {
+        const uint32_t w = ops[op0 + o];
+        apply_word<V, R, NV, GEN>(x, y, w, coefs[w >> kWordCoefShift], coefs, racc, lanes);
+      }
       // the store recomputes the offsets: without this the compiler keeps
       // all 2^R of them live across the ops for reuse, which costs registers
       // the amplitudes need
@@ -511,11 +520,13 @@ __global__ void __launch_bounds__(NT, MINB)
 }
 
 // Launch shapes.  A thread holds 2^R amplitudes per vector (64 registers
-// for complex<double> with R = 4, whose op switch needs ~190 registers in
-// all), so single-vector complex<double> runs CTAs of 128 threads, two per
-// SM by default (three with qsv_fuse_opts.ctas_per_sm = 3, at 168
-// registers); complex<float> with R = 4 runs 256-thread CTAs, three per SM
-// (two on request), with R = 5 two 128-thread CTAs.  Two-vector sweeps hold
+// for complex<double> with R = 4, whose op switch needs ~186 registers in
+// all), so single-vector complex<double> runs CTAs of 128 threads, three per
+// SM by default at 168 registers (two with qsv_fuse_opts.ctas_per_sm = 2:
+// measured 26 % slower on a 30-qubit brick of depth 40, 1186 against
+// 881 ms); complex<float> with R = 4 runs 256-thread CTAs, three per SM
+// (two on request), with R = 5 two 128-thread CTAs (three on request:
+// measured even).  Two-vector sweeps hold
 // 2 x 2^R amplitudes: R = 3 for complex<double>, 4 for complex<float>, in
 // 128-thread CTAs, three per SM (166 registers).  Each thread takes ngroups / threads
 // register groups per pass.
@@ -524,8 +535,8 @@ template <> struct GxKernels<double2> {
   static void* get(int R, int ctas, int nv, bool gen = false) {
     if (nv == 2)
       return gen ? (void*)k_gates<double2, 3, 128, 3, 2, true> : (void*)k_gates<double2, 3, 128, 3, 2>;
-    return ctas == 3 ? (void*)k_gates<double2, 4, 128, 3, 1>
-                     : (void*)k_gates<double2, 4, 128, 2, 1>;
+    return ctas == 2 ? (void*)k_gates<double2, 4, 128, 2, 1>
+                     : (void*)k_gates<double2, 4, 128, 3, 1>;
   }
   static int threads(int R, int nv) { (void)R; (void)nv; return 128; }
 };
@@ -533,7 +544,8 @@ template <> struct GxKernels<float2> {
   static void* get(int R, int ctas, int nv, bool gen = false) {
     if (nv == 2)
       return gen ? (void*)k_gates<float2, 4, 128, 3, 2, true> : (void*)k_gates<float2, 4, 128, 3, 2>;
-    if (R == 5) return (void*)k_gates<float2, 5, 128, 2, 1>;
+    if (R == 5)
+      return ctas == 3 ? (void*)k_gates<float2, 5, 128, 3, 1> : (void*)k_gates<float2, 5, 128, 2, 1>;
     return ctas == 2 ? (void*)k_gates<float2, 4, 256, 2, 1> : (void*)k_gates<float2, 4, 256, 3, 1>;
   }
   static int threads(int R, int nv) { return (nv == 2 || R == 5) ? 128 : 256; }

@@ -583,7 +583,9 @@ inline bool pack_gate_plan(const std::vector<Lowered>& gates, int n, int m, int 
       gp.nops = (int32_t)ops.size();
       for (size_t i = 0; i < ops.size(); ++i) {
         const GxOp& o = ops[i];
-        const size_t ci = out->coefs.size() - gs.coef0;
+        // ops without coefficients index entry 0 (the kernel loads every
+        // op's first coefficient one op ahead)
+        const size_t ci = o.ncoef ? out->coefs.size() - gs.coef0 : 0;
         if (ci >= (size_t(1) << (32 - kCodeBits))) return false;
         out->ops.push_back((uint32_t)o.code | ((uint32_t)ci << kCodeBits));
         for (int c = 0; c < o.ncoef; ++c) out->coefs.push_back(o.c[c]);
@@ -592,6 +594,7 @@ inline bool pack_gate_plan(const std::vector<Lowered>& gates, int n, int m, int 
     }
     gs.npasses = out->passes.size() - gs.pass0;
     gs.nops = out->ops.size() - gs.op0;
+    if (out->coefs.size() == gs.coef0) out->coefs.push_back(cplx(0.0, 0.0));  // entry 0
     gs.ncoef = out->coefs.size() - gs.coef0;
     out->stages.push_back(gs);
   }

@@ -38,5 +38,5 @@ def test_sweep_adjoint_and_batch(cuda):
 
 def test_sweep_kernels_workload(cuda):
     out = sweep.main(["--workload", "kernels", "--qubits", "12", "--repeat", "1"])
-    assert len(out["kernels"]) == 16
+    assert len(out["kernels"]) == 17
     assert all(v["ms"] > 0 for v in out["kernels"].values())
