@@ -15,8 +15,11 @@
 // A circuit whose two vectors fit in the CTA's shared memory (n <= m) never
 // touches global memory except for its results; larger circuits stream
 // their tiles through a per-CTA slot of a global workspace.  The stage and
-// pass plans come from the same planner as the single-state fused path
-// (stage_exec.cuh), packed for all circuits into one device buffer.
+// pass plans come from the same planner as the single-state fused path, and
+// the passes are the gate-specialised register passes (gate_plan.hpp,
+// gate_exec.cuh: every gate one op with compile-time register positions,
+// one-qubit gates factored to two multiply-adds per component), packed for
+// all circuits into one device buffer.
 // Gradient terms are summed by warp shuffles into a per-stage shared-memory
 // accumulator and added to the results once per stage, all in a fixed order,
 // so results are deterministic.
@@ -26,6 +29,8 @@
 #include <numeric>
 #include <vector>
 #include "fused.hpp"
+#include "gate_exec.cuh"
+#include "gate_plan.hpp"
 #include "stage_exec.cuh"
 
 using namespace qsv;
@@ -36,8 +41,9 @@ struct qsv_batch_s {
   int ncirc = 0;
   int tile_bits = 12;
   int blocks = 0;
-  int threads = 256;
+  int threads = 128;
   size_t smem = 0;
+  bool gen = false;           // backward stages hold generic gradient terms
   void* plan = nullptr;       // packed plan (device)
   size_t plan_bytes = 0;
   void* work = nullptr;       // per-CTA workspace (device)
@@ -65,7 +71,7 @@ namespace {
 
 struct BStage {          // one fused stage of one circuit
   int8_t bits[32];       // local tile bit -> global bit
-  int32_t m, full;
+  int32_t m, pad;
   int32_t pass0, npasses, op0, coef0;  // into the plan arrays (absolute)
   int32_t run0;                        // runoff offset (absolute)
   int32_t red0, nred;                  // gradient reductions: red_slots[red0..+nred)
@@ -101,8 +107,8 @@ struct BArgs {
   const BJob* jobs;
   int njobs;
   const BStage* stages;
-  const PassDev* passes;
-  const POp* ops;
+  const gx::GxPassDev* passes;
+  const uint32_t* ops;   // op words (gate_plan.hpp device_word)
   const void* coefs;
   const uint64_t* runoff;
   const BGroup* groups;
@@ -166,23 +172,26 @@ __device__ __forceinline__ TileArgs stage_tile(const BStage& S, int n, int low,
 }
 
 // One fused stage of a job on psi (NV = 1) or psi and lambda (NV = 2): the
-// stage's plan is staged in shared memory once, then every tile of the stage
-// is swept (the one resident tile of a circuit that fits shared memory).
-// Threads beyond the stage's 2^(m-R) register groups idle in the passes.
-template <typename V, int NV, int R>
+// stage's plan (pass descriptors | op words | coefficients) is staged in
+// shared memory once, then every tile of the stage is swept (the one
+// resident tile of a circuit that fits shared memory).  Threads beyond the
+// stage's 2^(m-R) register groups idle in the passes.
+template <typename V, int NV, int R, bool GEN>
 __device__ __forceinline__ void run_stage(const BStage& S, int n, int low, bool single,
                                           const BArgs& a, V* t0, V* t1, V* psi, V* lam,
                                           double* racc, unsigned char* plan, int rank = 0,
                                           int team = 1) {
-  const PassDev* passes;
-  const POp* ops;
-  const V* coefs;
-  stage_plan<V>(plan, a.passes + S.pass0, S.npasses, a.ops + S.op0, S.nops,
-                static_cast<const V*>(a.coefs) + S.coef0, S.ncoef, &passes, &ops, &coefs);
+  unsigned char* po = plan + align16(size_t(S.npasses) * sizeof(gx::GxPassDev));
+  unsigned char* pc = po + align16(size_t(S.nops) * sizeof(uint32_t));
+  copy_words(plan, a.passes + S.pass0, size_t(S.npasses) * sizeof(gx::GxPassDev));
+  copy_words(po, a.ops + S.op0, size_t(S.nops) * sizeof(uint32_t));
+  copy_words(pc, static_cast<const V*>(a.coefs) + S.coef0, size_t(S.ncoef) * sizeof(V));
   __syncthreads();
-  const uint32_t ngroups = 1u << (S.m - R);
+  const gx::GxPassDev* passes = reinterpret_cast<const gx::GxPassDev*>(plan);
+  const uint32_t* ops = reinterpret_cast<const uint32_t*>(po);
+  const V* coefs = reinterpret_cast<const V*>(pc);
   if (single) {
-    run_passes<V, NV, R, true, 0, true>(t0, t1, passes, S.npasses, ops, coefs, racc, ngroups);
+    gx::run_gate_passes<V, R, NV, GEN>(t0, t1, passes, S.npasses, ops, coefs, racc, S.m);
     return;
   }
   const TileArgs ta = stage_tile<V>(S, n, low, a.runoff);
@@ -191,7 +200,7 @@ __device__ __forceinline__ void run_stage(const BStage& S, int n, int low, bool 
     const uint64_t base = tile_base(ta, t);
     load_tile<V, NV>(psi, lam, t0, t1, ta, base, a.vec16);
     __syncthreads();
-    run_passes<V, NV, R, true, 0, true>(t0, t1, passes, S.npasses, ops, coefs, racc, ngroups);
+    gx::run_gate_passes<V, R, NV, GEN>(t0, t1, passes, S.npasses, ops, coefs, racc, S.m);
     store_tile<V, NV>(psi, lam, t0, t1, ta, base, a.vec16);
     __syncthreads();
   }
@@ -225,15 +234,14 @@ __device__ __forceinline__ double apply_group(const V* t0, V* t1, const BGroup& 
   return e;
 }
 
-// CTAs per SM the persistent kernel is compiled for: at 1 its ~200 registers
-// per thread need no spills; at 2 it spills about 300 bytes per thread but
-// runs the 4096-circuit batch 14 % faster (measured on a B200).
-#ifndef QSV_BATCH_MINBLOCKS
-#define QSV_BATCH_MINBLOCKS 2
-#endif
+// The persistent kernel runs CTAs of kBatchThreads threads, compiled for two
+// per SM (up to 255 registers a thread: the two-vector gate passes hold 2 x
+// 2^RB amplitudes plus the op dispatch's temporaries).  GEN: the backward
+// stages hold generic gradient terms (gate_exec.cuh red_generic).
+constexpr int kBatchThreads = 128;
 
-template <typename V, int RF, int RB>
-__global__ void __launch_bounds__(256, QSV_BATCH_MINBLOCKS)
+template <typename V, int RF, int RB, bool GEN>
+__global__ void __launch_bounds__(kBatchThreads, 2)
 k_batch(BArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double2 red[32];
@@ -297,8 +305,8 @@ k_batch(BArgs a) {
 
     // ---- forward ----
     for (int s = 0; s < J.nfwd; ++s) {
-      run_stage<V, 1, RF>(a.stages[J.fwd0 + s], J.n, J.low, single, a, t0, t1, psi, lam, racc,
-                          plan, rank, team);
+      run_stage<V, 1, RF, false>(a.stages[J.fwd0 + s], J.n, J.low, single, a, t0, t1, psi, lam,
+                                 racc, plan, rank, team);
       barrier();
     }
 
@@ -352,7 +360,8 @@ k_batch(BArgs a) {
     for (int s = 0; s < J.nbwd; ++s) {
       const BStage S = a.stages[J.bwd0 + s];
       for (int i = threadIdx.x; i < S.nred * kRedWarps; i += blockDim.x) racc[i] = 0.0;
-      run_stage<V, 2, RB>(S, J.n, J.low, single, a, t0, t1, psi, lam, racc, plan, rank, team);
+      run_stage<V, 2, RB, GEN>(S, J.n, J.low, single, a, t0, t1, psi, lam, racc, plan, rank,
+                               team);
       // the stage's gradient terms, summed over warps in a fixed order by one
       // thread (parameters may repeat within a stage)
       if (threadIdx.x == 0) {
@@ -383,6 +392,12 @@ k_batch(BArgs a) {
     }
     __syncthreads();
   }
+}
+
+template <typename V> V batch_coef(gx::cplx z);
+template <> double2 batch_coef<double2>(gx::cplx z) { return make_double2(z.real(), z.imag()); }
+template <> float2 batch_coef<float2>(gx::cplx z) {
+  return make_float2((float)z.real(), (float)z.imag());
 }
 
 template <typename V>
@@ -430,7 +445,12 @@ qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate*
   const size_t smem = (size_t(2) << M) * sizeof(V) + kRaccBytes + kPlanSmemMax;
   if (smem > 200 * 1024) return fail(QSV_ERROR_SIZE, "batch tiles exceed shared memory");
 
-  PackedPlan<V> plan;
+  PackedPlan<V> plan;  // run offsets of stages and term groups
+  std::vector<gx::GxPassDev> gpasses;
+  std::vector<uint32_t> gops;
+  std::vector<V> gcoefs;
+  std::vector<int32_t> gred;
+  bool gen = false;
   std::vector<BStage> stages;
   std::vector<BGroup> groups;
   std::vector<BTerm> terms;
@@ -490,32 +510,65 @@ qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate*
     b->grad_off[c] = goff - ncirc;
     b->nparams[c] = nparams[c];
     goff += nparams[c];
-    auto pack = [&](const std::vector<Lowered>& items, int r, int32_t* first, int32_t* count) {
-      const size_t s0 = plan.stages.size();
-      if (qsv_status st = pack_plan<V>(items, n, m, lo, r, 256, &plan)) return st;
+    // gate-specialised plan of one direction -> device stages, passes (with
+    // their shared-memory offsets for the cp.async tile layout), op words,
+    // coefficients and gradient rows
+    auto pack = [&](const std::vector<Lowered>& items, int r, bool two, int32_t* first,
+                    int32_t* count) -> qsv_status {
+      gx::GxPlan gp;
+      if (!gx::pack_gate_plan(items, n, m, lo, r, 256, kPlanSmemMax, sizeof(V), &gp, two))
+        return fail(QSV_ERROR_NOT_SUPPORTED, "circuit %d: a gate cannot run in a batched sweep", c);
       *first = (int32_t)stages.size();
-      for (size_t si = s0; si < plan.stages.size(); ++si) {
-        const PackedStage& ps = plan.stages[si];
+      const uint32_t rdg = (uint32_t)gx::code_red(r, gx::G_RDG, 0);
+      for (const gx::GxStage& gs : gp.stages) {
         BStage S{};
-        for (int j = 0; j < 32; ++j) S.bits[j] = (int8_t)(j < ps.m ? ps.bits[j] : 0);
-        S.m = ps.m;
-        S.full = ps.full;
-        S.pass0 = (int32_t)ps.pass0;
-        S.npasses = (int32_t)ps.npasses;
-        S.op0 = (int32_t)ps.op0;
-        S.coef0 = (int32_t)ps.coef0;
-        S.run0 = (int32_t)ps.run0;
-        S.red0 = (int32_t)ps.red0;
-        S.nred = ps.nred;
-        S.nops = ps.nops;
-        S.ncoef = ps.ncoef;
+        for (int j = 0; j < 32; ++j) S.bits[j] = (int8_t)(j < gs.m ? gs.bits[j] : 0);
+        S.m = gs.m;
+        S.pass0 = (int32_t)gpasses.size();
+        S.npasses = (int32_t)gs.npasses;
+        S.op0 = (int32_t)gops.size();
+        S.nops = (int32_t)gs.nops;
+        S.coef0 = (int32_t)gcoefs.size();
+        S.ncoef = (int32_t)gs.ncoef;
+        S.red0 = (int32_t)gred.size();
+        S.nred = gs.nred;
+        S.run0 = (int32_t)plan.runoff.size();
+        tile_runoffs(gs.bits, gs.m, lo, &plan.runoff);
+        if (gx::gx_plan_smem<V>(gs.npasses, gs.nops, gs.ncoef) > kPlanSmemMax)
+          return fail(QSV_ERROR_SIZE, "circuit %d: a stage plan exceeds shared memory", c);
+        for (size_t pi = gs.pass0; pi < gs.pass0 + gs.npasses; ++pi) {
+          const gx::GxPass& q = gp.passes[pi];
+          gx::GxPassDev d{};
+          int pos[8];
+          for (int k = 0; k < 8; ++k) {
+            d.pos[k] = q.pos[k];
+            pos[k] = q.pos[k];
+          }
+          d.op0 = q.op0;
+          d.nops = q.nops;
+          for (int k = 0; k < r; ++k) d.boff[k] = phys_host(1u << pos[k], Units<V>::per);
+          int order[32];
+          const int ng = gx::lane_order(pos, r, gs.m, sizeof(V), order, -1);
+          if (ng > 12) return fail(QSV_ERROR_SIZE, "circuit %d: stage of %d tile bits", c, gs.m);
+          for (int k = 0; k < ng; ++k) d.goff[k] = phys_host(1u << order[k], Units<V>::per);
+          gpasses.push_back(d);
+        }
+        for (size_t o = gs.op0; o < gs.op0 + gs.nops; ++o) {
+          const uint32_t w = gp.ops[o];
+          const uint32_t code = w & ((1u << gx::kCodeBits) - 1u);
+          if (two && code == rdg) gen = true;
+          gops.push_back(gx::device_word((int)code, r, w >> gx::kCodeBits));
+        }
+        for (size_t k = gs.coef0; k < gs.coef0 + gs.ncoef; ++k)
+          gcoefs.push_back(batch_coef<V>(gp.coefs[k]));
+        for (int k = 0; k < gs.nred; ++k) gred.push_back(gp.red_slots[gs.red0 + k]);
         stages.push_back(S);
       }
       *count = (int32_t)(stages.size() - *first);
       return QSV_SUCCESS;
     };
-    if (qsv_status st = pack(fwd, RF, &J.fwd0, &J.nfwd)) return st;
-    if (qsv_status st = pack(bwd, RB, &J.bwd0, &J.nbwd)) return st;
+    if (qsv_status st = pack(fwd, RF, false, &J.fwd0, &J.nfwd)) return st;
+    if (qsv_status st = pack(bwd, RB, true, &J.bwd0, &J.nbwd)) return st;
     // observable term groups (flip bits within an m-bit tile)
     std::vector<HTermH> H;
     const size_t nt = term_off[c + 1] - term_off[c];
@@ -577,13 +630,15 @@ qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate*
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (qsv_status st = cuda_status(cudaFuncSetAttribute(k_batch<V, RF, RB>,
+  void* kern = gen ? (void*)k_batch<V, RF, RB, true> : (void*)k_batch<V, RF, RB, false>;
+  if (qsv_status st = cuda_status(cudaFuncSetAttribute(kern,
                                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                        (int)smem), "batch smem attribute"))
     return st;
   int per_sm = 0;
-  const int threads = 1 << (M - RB) < 32 ? 32 : 1 << (M - RB);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<V, RF, RB>, threads, smem);
+  // one thread per register group of the widest pass, kBatchThreads at most
+  const int threads = std::max(32, std::min(kBatchThreads, 1 << (M - std::min(RF, RB))));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
   if (opts && opts->ctas_per_sm > 0) per_sm = std::min(per_sm, opts->ctas_per_sm);
   if (per_sm < 1) return fail(QSV_ERROR_NOT_SUPPORTED, "batch kernel does not fit an SM");
   int blocks = sms * per_sm;
@@ -629,28 +684,29 @@ qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate*
   size_t off = 0;
   b->off_jobs = off;   off = align(off + jobs.size() * sizeof(BJob));
   b->off_stages = off; off = align(off + stages.size() * sizeof(BStage));
-  b->off_passes = off; off = align(off + plan.passes.size() * sizeof(PassDev));
-  b->off_ops = off;    off = align(off + plan.ops.size() * sizeof(POp));
-  b->off_coefs = off;  off = align(off + plan.coefs.size() * sizeof(V));
+  b->off_passes = off; off = align(off + gpasses.size() * sizeof(gx::GxPassDev));
+  b->off_ops = off;    off = align(off + gops.size() * sizeof(uint32_t));
+  b->off_coefs = off;  off = align(off + gcoefs.size() * sizeof(V));
   b->off_runoff = off; off = align(off + plan.runoff.size() * sizeof(uint64_t));
   b->off_groups = off; off = align(off + groups.size() * sizeof(BGroup));
   b->off_terms = off;  off = align(off + terms.size() * sizeof(BTerm));
-  b->off_red = off;    off = align(off + plan.red_slots.size() * sizeof(int32_t));
+  b->off_red = off;    off = align(off + gred.size() * sizeof(int32_t));
   std::vector<unsigned char> host(off, 0);
   auto put = [&](size_t o, const void* p, size_t bytes) { if (bytes) std::memcpy(host.data() + o, p, bytes); };
   put(b->off_jobs, jobs.data(), jobs.size() * sizeof(BJob));
   put(b->off_stages, stages.data(), stages.size() * sizeof(BStage));
-  put(b->off_passes, plan.passes.data(), plan.passes.size() * sizeof(PassDev));
-  put(b->off_ops, plan.ops.data(), plan.ops.size() * sizeof(POp));
-  put(b->off_coefs, plan.coefs.data(), plan.coefs.size() * sizeof(V));
+  put(b->off_passes, gpasses.data(), gpasses.size() * sizeof(gx::GxPassDev));
+  put(b->off_ops, gops.data(), gops.size() * sizeof(uint32_t));
+  put(b->off_coefs, gcoefs.data(), gcoefs.size() * sizeof(V));
   put(b->off_runoff, plan.runoff.data(), plan.runoff.size() * sizeof(uint64_t));
   put(b->off_groups, groups.data(), groups.size() * sizeof(BGroup));
   put(b->off_terms, terms.data(), terms.size() * sizeof(BTerm));
-  put(b->off_red, plan.red_slots.data(), plan.red_slots.size() * sizeof(int32_t));
+  put(b->off_red, gred.data(), gred.size() * sizeof(int32_t));
 
   // every CTA can hold a team member, but a grid smaller than the jobs is enough
   b->blocks = std::min<int>(blocks, b->njobs);
   b->threads = threads;
+  b->gen = gen;
   b->smem = smem;
   b->tile_bits = M;
   b->work_bytes = (nmax > M) ? (size_t)b->blocks * stride * sizeof(V) : 256;
@@ -682,8 +738,8 @@ qsv_status launch_batch(qsv_batch_s* b, cudaStream_t stream) {
   a.jobs = reinterpret_cast<const BJob*>(p + b->off_jobs);
   a.njobs = b->njobs;
   a.stages = reinterpret_cast<const BStage*>(p + b->off_stages);
-  a.passes = reinterpret_cast<const PassDev*>(p + b->off_passes);
-  a.ops = reinterpret_cast<const POp*>(p + b->off_ops);
+  a.passes = reinterpret_cast<const gx::GxPassDev*>(p + b->off_passes);
+  a.ops = reinterpret_cast<const uint32_t*>(p + b->off_ops);
   a.coefs = p + b->off_coefs;
   a.runoff = reinterpret_cast<const uint64_t*>(p + b->off_runoff);
   a.groups = reinterpret_cast<const BGroup*>(p + b->off_groups);
@@ -703,7 +759,10 @@ qsv_status launch_batch(qsv_batch_s* b, cudaStream_t stream) {
   if (qsv_status st = cuda_status(cudaMemsetAsync(b->results, 0, b->zero_bytes, stream),
                                   "batch results reset"))
     return st;
-  k_batch<V, RF, RB><<<b->blocks, b->threads, b->smem, stream>>>(a);
+  if (b->gen)
+    k_batch<V, RF, RB, true><<<b->blocks, b->threads, b->smem, stream>>>(a);
+  else
+    k_batch<V, RF, RB, false><<<b->blocks, b->threads, b->smem, stream>>>(a);
   count_launch();
   return cuda_status(cudaGetLastError(), "batch kernel launch");
 }
