@@ -223,6 +223,7 @@ def batch_extra(torch, stream, ncirc=4096, seed=21, check=16, loop_sample=64):
     from qclab_b200.batch import Batch, autotune
     from qclab_b200.gradients import adjoint_gradient
     from qclab_b200.observable import ising
+    peak, peak_kind = peaks()
     rng = np.random.default_rng(seed)
     ns = rng.integers(8, 19, size=ncirc)
     ls = rng.integers(4, 17, size=ncirc)
@@ -241,7 +242,9 @@ def batch_extra(torch, stream, ncirc=4096, seed=21, check=16, loop_sample=64):
         torch.cuda.synchronize()
         return ev[0].elapsed_time(ev[1]) / reps / 1e3
 
-    cands = [{"tile_bits": m, "low_bits": 2, "ctas_per_sm": c} for m in (10, 11, 12) for c in (0, 1, 2)]
+    # the persistent kernel fits at most two CTAs per SM: 0 (the occupancy
+    # limit) and 1 are the distinct choices
+    cands = [{"tile_bits": m, "low_bits": 2, "ctas_per_sm": c} for m in (10, 11, 12) for c in (0, 1)]
     t0 = time.perf_counter()
     best, times = autotune(circs, obs, np.complex64, cands=cands, timer=ev_timer,
                            cache=Path(tempfile.mkdtemp()) / "tune.json")
@@ -254,6 +257,7 @@ def batch_extra(torch, stream, ncirc=4096, seed=21, check=16, loop_sample=64):
         e, g = b.results(s)
         e2e = time.perf_counter() - t0
         info = b.info()
+        work = b.work()
     idx = list(range(0, ncirc, max(1, ncirc // check)))[:check]
     err_e = err_g = 0.0
     for i in idx:
@@ -282,6 +286,14 @@ def batch_extra(torch, stream, ncirc=4096, seed=21, check=16, loop_sample=64):
             "launch_ms": sec * 1e3, "circuits_per_s": ncirc / sec,
             "angle_derivatives_per_s": nparams / sec, "e2e_ms_with_results_copy": e2e * 1e3,
             "autotuned": best, "autotune_s": tune_s,
+            "amplitude_updates_per_s": work["amplitude_updates"] / sec,
+            "roofline": {"bound": "hbm", "achieved": work["global_bytes"] / sec / 1e9,
+                         "peak": peak, "unit": "GB/s",
+                         "frac": work["global_bytes"] / sec / 1e9 / peak,
+                         "peak_source": f"{peak_kind} hbm_gbs",
+                         "traffic_note": "tile traffic of the circuits larger than a tile "
+                                         "(the others stay in shared memory): "
+                                         f"{work['global_bytes'] / 1e9:.2f} GB per launch"},
             "autotune_ms": {k: v * 1e3 for k, v in times.items()}, "launch_shape": info,
             "max_abs_energy_err_vs_c128": err_e, "max_abs_grad_err_vs_c128": err_g,
             "checked_circuits": len(idx),

@@ -327,6 +327,13 @@ qsv_status qsv_batch_results(qsv_batch batch, void* cuda_stream,
                              double* energies, double* gradients);
 qsv_status qsv_batch_info(qsv_batch batch, int* blocks, int* threads,
                           int* tile_bits, size_t* workspace_bytes);
+/* Work of one launch, from the plan: global_bytes = tile traffic of the
+ * circuits larger than a tile (each stage reads and writes its vectors once;
+ * circuits that fit a tile stay in shared memory and move none);
+ * amplitude_updates = sum over circuits of 2^n x (forward gates + 2 x
+ * backward gates).  Either pointer may be NULL. */
+qsv_status qsv_batch_work(qsv_batch batch, double* global_bytes,
+                          double* amplitude_updates);
 qsv_status qsv_batch_destroy(qsv_batch batch);
 
 /* ---- device probe (new) --------------------------------------------------

@@ -122,6 +122,7 @@ def _declare(lib):
         "qsv_batch_run": ([p, p, i], i),
         "qsv_batch_results": ([p, p, p, p], i),
         "qsv_batch_info": ([p, C.POINTER(i), C.POINTER(i), C.POINTER(i), C.POINTER(sz)], i),
+        "qsv_batch_work": ([p, C.POINTER(C.c_double), C.POINTER(C.c_double)], i),
         "qsv_batch_destroy": ([p], i),
         "qsv_set_identity": ([p], i),
         "qsv_apply_matrix": ([p, gp, sz, C.c_char, C.c_char, i, i], i),

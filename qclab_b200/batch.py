@@ -106,6 +106,13 @@ class Batch:
         return {"blocks": b.value, "threads": t.value, "tile_bits": m.value,
                 "workspace_bytes": w.value}
 
+    def work(self) -> dict:
+        """Work of one launch from the plan (``qsv_batch_work``): global tile
+        traffic in bytes and gate x amplitude updates."""
+        gb, au = C.c_double(), C.c_double()
+        L.check(self._lib.qsv_batch_work(self.handle, C.byref(gb), C.byref(au)), "qsv_batch_work")
+        return {"global_bytes": gb.value, "amplitude_updates": au.value}
+
     def close(self) -> None:
         if getattr(self, "_h", None) is not None:
             self._lib.qsv_batch_destroy(self._h)

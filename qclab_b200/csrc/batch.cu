@@ -44,6 +44,8 @@ struct qsv_batch_s {
   int threads = 128;
   size_t smem = 0;
   bool gen = false;           // backward stages hold generic gradient terms
+  double global_bytes = 0;    // per launch: tile traffic of the circuits larger than a tile
+  double amp_updates = 0;     // per launch: gate x amplitude updates (both vectors)
   void* plan = nullptr;       // packed plan (device)
   size_t plan_bytes = 0;
   void* work = nullptr;       // per-CTA workspace (device)
@@ -569,6 +571,14 @@ qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate*
     };
     if (qsv_status st = pack(fwd, RF, false, &J.fwd0, &J.nfwd)) return st;
     if (qsv_status st = pack(bwd, RB, true, &J.bwd0, &J.nbwd)) return st;
+    {  // work of this circuit: every gate updates 2^n amplitudes (forward),
+       // 2 x 2^n backward (psi and lambda)
+      size_t nf = 0, nb = 0;
+      for (const Lowered& L : fwd) nf += L.shape != SH_NONE;
+      for (const Lowered& L : bwd) nb += L.shape != SH_NONE && L.shape != SH_RED;
+      const double N = (double)(1ull << n);
+      b->amp_updates += N * (double)(nf + 2 * nb);
+    }
     // observable term groups (flip bits within an m-bit tile)
     std::vector<HTermH> H;
     const size_t nt = term_off[c + 1] - term_off[c];
@@ -619,6 +629,12 @@ qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate*
         terms.push_back(T);
       }
       groups.push_back(G);
+    }
+    if (n > m) {  // streamed through the workspace: every stage reads and
+                  // writes its vector(s) once, a term group reads psi (and
+                  // lambda after the first) and writes lambda
+      const double vb = (double)(1ull << n) * sizeof(V);
+      b->global_bytes += vb * (2.0 * J.nfwd + 4.0 * J.nbwd + 2.0 + 3.0 * (J.ngrp - 1));
     }
     jobs.push_back(J);
   }
@@ -881,6 +897,13 @@ qsv_status qsv_batch_info(qsv_batch b, int* blocks, int* threads, int* tile_bits
   if (threads) *threads = b->threads;
   if (tile_bits) *tile_bits = b->tile_bits;
   if (workspace_bytes) *workspace_bytes = b->work_bytes;
+  return QSV_SUCCESS;
+}
+
+qsv_status qsv_batch_work(qsv_batch b, double* global_bytes, double* amplitude_updates) {
+  if (!b) return fail(QSV_ERROR_INVALID_VALUE, "null batch");
+  if (global_bytes) *global_bytes = b->global_bytes;
+  if (amplitude_updates) *amplitude_updates = b->amp_updates;
   return QSV_SUCCESS;
 }
 

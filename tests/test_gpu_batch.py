@@ -114,6 +114,12 @@ def test_graph_replay_is_deterministic(cuda):
             assert all(np.array_equal(x, y) for x, y in zip(g0, g1))
         info = b.info()
         assert info["tile_bits"] == 11 and info["blocks"] >= 1
+        # work of one launch from the plan: every gate updates 2^n amplitudes
+        # forward and 2 x 2^n backward; only the 12- and 14-qubit circuits
+        # (larger than the 11-bit tiles) move tiles through global memory
+        work = b.work()
+        assert work["amplitude_updates"] == sum(3 * len(c) * 2 ** n for c, n in zip(circs, ns))
+        assert work["global_bytes"] >= sum(8 * 2 ** n * 6 for n in ns if n > 11)
 
 
 def test_shared_parameters_accumulate(cuda):
