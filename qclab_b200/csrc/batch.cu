@@ -241,9 +241,12 @@ __device__ __forceinline__ double apply_group(const V* t0, V* t1, const BGroup& 
 // 2^RB amplitudes plus the op dispatch's temporaries).  GEN: the backward
 // stages hold generic gradient terms (gate_exec.cuh red_generic).
 constexpr int kBatchThreads = 128;
+#ifndef QSV_BATCH_MINBLOCKS
+#define QSV_BATCH_MINBLOCKS 2
+#endif
 
 template <typename V, int RF, int RB, bool GEN>
-__global__ void __launch_bounds__(kBatchThreads, 2)
+__global__ void __launch_bounds__(kBatchThreads, QSV_BATCH_MINBLOCKS)
 k_batch(BArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double2 red[32];

@@ -290,23 +290,24 @@ __device__ __forceinline__ void red_op(const V (&x)[N], const V (&y)[N], const V
     return;
   }
   constexpr int M = 1 << P;
-  double sr = 0.0, si = 0.0;
+  // only the part the term needs (RDY: Re, else Im), one independent signed
+  // product per register, then a pairwise sum: a dependency chain of
+  // log2(2^R) additions instead of 2^R (the sweep is latency-bound here)
+  double v[N];
 #pragma unroll
   for (int j = 0; j < N; ++j) {
     const int f = (K == G_RDZ) ? j : (j ^ M);
     const bool neg = (K == G_RDY) ? ((f & M) != 0) : (K == G_RDZ) ? ((j & M) != 0) : false;
     const double2 a = to_d2(y[j]), b = to_d2(x[f]);
-    const double re = fma(a.x, b.x, a.y * b.y), im = fma(a.x, b.y, -a.y * b.x);
-    if (neg) {
-      sr -= re;
-      si -= im;
-    } else {
-      sr += re;
-      si += im;
-    }
+    const double t = (K == G_RDY) ? fma(a.x, b.x, a.y * b.y) : fma(a.x, b.y, -a.y * b.x);
+    v[j] = neg ? -t : t;
   }
+#pragma unroll
+  for (int h = 1; h < N; h <<= 1)
+#pragma unroll
+    for (int j = 0; j < N; j += 2 * h) v[j] += v[j + h];
   const double2 cc = to_d2(cw);
-  fx::red_accumulate(cc.x * ((K == G_RDY) ? sr : si), (int)cc.y, racc, lanes);
+  fx::red_accumulate(cc.x * v[0], (int)cc.y, racc, lanes);
 }
 
 // One op word (device_word in gate_plan.hpp): kind (bits 0-4), register

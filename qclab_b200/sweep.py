@@ -147,7 +147,9 @@ def _batch(a) -> dict:
     obs = [ising(int(n)) for n in ns]
     out = {"workload": "batch", "circuits": a.circuits, "dtype": a.dtype,
            "gates": int(sum(len(c.gate_records(dt)) for c in circs))}
-    with Batch(circs, obs, dt) as b:
+    with Batch(circs, obs, dt, tile_bits=a.tile_bits, ctas_per_sm=a.ctas_per_sm) as b:
+        out["launch_shape"] = b.info()
+
         def run():
             b.run()
             b.results()
