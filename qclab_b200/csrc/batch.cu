@@ -236,13 +236,17 @@ __device__ __forceinline__ double apply_group(const V* t0, V* t1, const BGroup& 
   return e;
 }
 
-// The persistent kernel runs CTAs of kBatchThreads threads, compiled for two
-// per SM (up to 255 registers a thread: the two-vector gate passes hold 2 x
-// 2^RB amplitudes plus the op dispatch's temporaries).  GEN: the backward
+// The persistent kernel runs CTAs of kBatchThreads threads, compiled for
+// three per SM (168 registers a thread: the two-vector gate passes hold 2 x
+// 2^RB amplitudes plus the op dispatch's temporaries; complex<float> spills
+// about 70 bytes).  Shared memory admits three with 2^11-amplitude tiles
+// (two with 2^12): on the 4096-circuit batch 2^11 tiles at three CTAs per SM
+// took 265-270 ms against 286-289 ms with 2^12 tiles at two (compiled for
+// two per SM, 236 registers, no spills: the same 288 ms).  GEN: the backward
 // stages hold generic gradient terms (gate_exec.cuh red_generic).
 constexpr int kBatchThreads = 128;
 #ifndef QSV_BATCH_MINBLOCKS
-#define QSV_BATCH_MINBLOCKS 2
+#define QSV_BATCH_MINBLOCKS 3
 #endif
 
 template <typename V, int RF, int RB, bool GEN>
@@ -443,7 +447,7 @@ qsv_status build_batch(qsv_batch_s* b, int ncirc, const int* nq, const qsv_gate*
                        const double* coefs, const size_t* term_off, const int* nparams,
                        const qsv_batch_opts* opts) {
   constexpr int RF = fwd_bits<V>(), RB = bwd_bits<V>();
-  const int M = (opts && opts->tile_bits > 0) ? opts->tile_bits : (sizeof(V) >= 16 ? 11 : 12);
+  const int M = (opts && opts->tile_bits > 0) ? opts->tile_bits : 11;
   const int low = (opts && opts->low_bits > 0) ? opts->low_bits : default_low_bits(sizeof(V));
   if (M < RF || M - RB > 8 || M > 14)
     return fail(QSV_ERROR_INVALID_VALUE, "batch tile_bits %d outside [%d, %d]", M, RF, RB + 8);

@@ -292,14 +292,19 @@ __device__ __forceinline__ void red_op(const V (&x)[N], const V (&y)[N], const V
   constexpr int M = 1 << P;
   // only the part the term needs (RDY: Re, else Im), one independent signed
   // product per register, then a pairwise sum: a dependency chain of
-  // log2(2^R) additions instead of 2^R (the sweep is latency-bound here)
-  double v[N];
+  // log2(2^R) additions instead of 2^R (the sweep is latency-bound here).
+  // complex<float>: products and this in-thread sum in float (the amplitudes
+  // carry float rounding already; converting every operand to double cost
+  // four conversions per register on the slow conversion pipe), one
+  // conversion per term; the sums across lanes, tiles and the state are FP64.
+  using T = typename RealOf<V>::T;
+  T v[N];
 #pragma unroll
   for (int j = 0; j < N; ++j) {
     const int f = (K == G_RDZ) ? j : (j ^ M);
     const bool neg = (K == G_RDY) ? ((f & M) != 0) : (K == G_RDZ) ? ((j & M) != 0) : false;
-    const double2 a = to_d2(y[j]), b = to_d2(x[f]);
-    const double t = (K == G_RDY) ? fma(a.x, b.x, a.y * b.y) : fma(a.x, b.y, -a.y * b.x);
+    const V a = y[j], b = x[f];
+    const T t = (K == G_RDY) ? fma(a.x, b.x, a.y * b.y) : fma(a.x, b.y, -a.y * b.x);
     v[j] = neg ? -t : t;
   }
 #pragma unroll
@@ -307,7 +312,7 @@ __device__ __forceinline__ void red_op(const V (&x)[N], const V (&y)[N], const V
 #pragma unroll
     for (int j = 0; j < N; j += 2 * h) v[j] += v[j + h];
   const double2 cc = to_d2(cw);
-  fx::red_accumulate(cc.x * v[0], (int)cc.y, racc, lanes);
+  fx::red_accumulate(cc.x * (double)v[0], (int)cc.y, racc, lanes);
 }
 
 // One op word (device_word in gate_plan.hpp): kind (bits 0-4), register
