@@ -15,5 +15,6 @@ from .gates import (QObject, QGate1, QGate2, QControlledGate2, Identity, Hadamar
                     CPhase, CRotationX, CRotationY, CRotationZ)
 from .circuit import QCircuit
 from .state import StateVector, launch_count, tma_launch_count
+from .sharded import ShardedStateVector
 
 __all__ = [n for n in dir() if not n.startswith("_")]
