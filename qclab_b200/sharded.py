@@ -95,6 +95,8 @@ class ShardedStateVector:
             device = (torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
                       if engine is None else torch.device("cpu"))
         self.device = torch.device(device)
+        if self.device.type == "cuda":  # NCCL's point-to-point calls need the device current
+            torch.cuda.set_device(self.device)
         self.buf = torch.zeros(1 << self.nl, dtype=tdt, device=self.device)
         self.stage = torch.empty(1 << (self.nl - 1), dtype=tdt, device=self.device)
         if self.rank == 0:
