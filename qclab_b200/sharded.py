@@ -57,6 +57,10 @@ class CudaEngine:
     def norm2(self) -> float:
         return self.sv.norm2()
 
+    def expectation(self, paulis, coefs) -> float:
+        from .observable import Observable
+        return self.sv.expectation(Observable(self.sv.nbQubits, zip(coefs, paulis)))
+
     def synchronize(self) -> None:
         self.sv.synchronize()
 
@@ -192,6 +196,62 @@ class ShardedStateVector:
         flush()
 
     # ---- reductions and host copies ----------------------------------------------------
+    def expectation(self, obs) -> float:
+        """<psi|H|psi> in FP64 for a Pauli sum (``observable.Observable`` on
+        the logical qubits; a term may hold at most n - g X/Y factors).  A
+        term's X and Y factors on qubits in global slots are first moved into
+        the local state (the gates' exchanges); a Z on a global slot is this
+        rank's sign.  Terms between two exchanges
+        are evaluated by one library call on the local state; the ranks' sums
+        are all-reduced."""
+        import torch
+        if obs.nbQubits != self.n:
+            raise ValueError("observable and state sizes differ")
+        total = 0.0
+        loc_p: list[str] = []
+        loc_c: list[float] = []
+
+        def flush():
+            nonlocal total
+            if loc_p:
+                total += self.engine.expectation(list(loc_p), list(loc_c))
+                loc_p.clear()
+                loc_c.clear()
+
+        for coef, pstr in zip(obs.coefs, obs.paulis):
+            support = [q for q, c in enumerate(pstr) if c != "I"]
+            flips = [q for q in support if pstr[q] in "XY"]
+            if len(flips) > self.nl:
+                raise ValueError(f"a term with {len(flips)} X/Y factors does not fit "
+                                 f"{self.nl} local qubits")
+            for q in flips:
+                p = self.slot_of[q]
+                if p >= self.g:
+                    continue
+                flush()
+                # the top local slot must not hold another X/Y qubit of the
+                # term (a Z qubit may go to a rank's slot: it becomes a sign)
+                used = {self.slot_of[x] for x in flips}
+                if self.g in used:
+                    t = next(s for s in range(self.g + 1, self.n) if s not in used)
+                    self._local_swap(self.g, t)
+                self._exchange(p)
+            local = ["I"] * self.nl
+            sign = 1.0
+            for q in support:
+                s = self.slot_of[q]
+                if s >= self.g:
+                    local[s - self.g] = pstr[q]
+                elif (self.rank >> (self.g - 1 - s)) & 1:  # a Z on this rank's bit 1
+                    sign = -sign
+            loc_p.append("".join(local))
+            loc_c.append(sign * coef)
+        flush()
+        t = torch.tensor([total], dtype=torch.float64,
+                         device=self.device if self.backend == "nccl" else "cpu")
+        self.dist.all_reduce(t, group=self.group)
+        return float(t.item())
+
     def norm2(self) -> float:
         """<psi|psi> in FP64: the local sums, then one all-reduce."""
         import torch

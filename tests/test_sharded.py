@@ -38,6 +38,9 @@ class OracleEngine:
     def norm2(self):
         return float(np.vdot(self.x, self.x).real)
 
+    def expectation(self, paulis, coefs):
+        return oracle.expectation(self.x, list(zip(coefs, paulis)))
+
     def synchronize(self):
         pass
 
@@ -48,6 +51,21 @@ class OracleEngine:
 def _circuit(n, seed):
     c = W.random_mixed(n, 90, seed=seed)
     return c.gate_records(np.complex128)
+
+
+def _observable(n):
+    """Ising chain plus strings with X, Y and Z on the ranks' top qubits."""
+    from qclab_b200.observable import ising
+    H = ising(n)
+    rng = np.random.default_rng(9)
+    for _ in range(8):
+        t = ["I"] * n
+        for q in rng.choice(n, size=4, replace=False):
+            t[q] = "XYZ"[rng.integers(3)]
+        H.add(float(rng.normal()), "".join(t))
+    H.add(0.7, "XY" + "Z" * (n - 2))
+    H.add(-0.3, "ZZ" + "X" * (n - 2))
+    return H
 
 
 def _rank_main(rank, world, port, out, n, use_gpu):
@@ -69,9 +87,10 @@ def _rank_main(rank, world, port, out, n, use_gpu):
                     s.upload(x0)
                     s.apply(recs, op, fused=fused)
                     n2 = s.norm2()
+                    e = s.expectation(_observable(n))
                     y = s.download()
                     if rank == 0:
-                        res[(op, fused)] = (y, n2, s.exchanges)
+                        res[(op, fused)] = (y, n2, s.exchanges, e)
         with ShardedStateVector(n, np.complex128, **kw) as s:   # |0...0> start
             s.apply(recs[:30], "N")
             y = s.download()
@@ -106,11 +125,13 @@ def test_sharded_state_matches_whole_vector(world):
     n = 7
     res = _run(world, n, use_gpu=False)
     for op in ("N", "T", "C"):
-        y, n2, ex = res[str((op, False))]
+        y, n2, ex, e = res[str((op, False))]
         want = _expected(n, op)
         assert np.max(np.abs(y - want)) <= 1e-13, op
         assert ex > 0                      # the circuit touches the ranks' qubits
         assert abs(n2 - float(np.vdot(want, want).real)) < 1e-12
+        e_want = oracle.expectation(want, _observable(n).matrix_free_terms())
+        assert abs(e - e_want) <= 1e-12 * max(1.0, abs(e_want)), (op, e, e_want)
     z = np.zeros(1 << n, dtype=np.complex128)
     z[0] = 1
     assert np.max(np.abs(res["zero"] - oracle.apply(z, _circuit(n, 11)[:30], "N"))) <= 1e-13
@@ -131,8 +152,10 @@ def test_sharded_state_on_the_gpu(cuda):
     res = _run(2, n, use_gpu=True)
     for op in ("N", "T", "C"):
         want = _expected(n, op)
-        y, n2, ex = res[str((op, False))]
+        y, n2, ex, e = res[str((op, False))]
         assert np.max(np.abs(y - want)) <= 1e-13, op
         assert ex > 0
-        yf, _, _ = res[str((op, True))]
+        e_want = oracle.expectation(want, _observable(n).matrix_free_terms())
+        assert abs(e - e_want) <= 1e-12 * max(1.0, abs(e_want)), (op, e, e_want)
+        yf, _, _, _ = res[str((op, True))]
         assert np.max(np.abs(yf - want)) <= 1e-12, op
