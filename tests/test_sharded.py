@@ -1,4 +1,4 @@
-"""One state split over 2 and 4 ranks (``qclab_b200.sharded``): the gate
+"""One state split over 2, 4 and 8 ranks (``qclab_b200.sharded``): the gate
 list runs on the local states with pairwise half-state exchanges for gates
 on the ranks' qubits, and the state downloaded in logical order must equal
 the oracle applied to the whole vector.  On CPU the ranks are gloo
@@ -64,7 +64,7 @@ def _observable(n):
             t[q] = "XYZ"[rng.integers(3)]
         H.add(float(rng.normal()), "".join(t))
     H.add(0.7, "XY" + "Z" * (n - 2))
-    H.add(-0.3, "ZZ" + "X" * (n - 2))
+    H.add(-0.3, "ZZZ" + "X" * (n - 3))
     return H
 
 
@@ -120,9 +120,8 @@ def _expected(n, op, x0=None):
     return oracle.apply(x0.copy(), _circuit(n, 11), op)
 
 
-@pytest.mark.parametrize("world", [2, 4])
-def test_sharded_state_matches_whole_vector(world):
-    n = 7
+@pytest.mark.parametrize("world, n", [(2, 7), (4, 7), (8, 8)])
+def test_sharded_state_matches_whole_vector(world, n):
     res = _run(world, n, use_gpu=False)
     for op in ("N", "T", "C"):
         y, n2, ex, e = res[str((op, False))]
