@@ -100,6 +100,21 @@ def adjoint_extra(torch, stream, ps_params, fd_params=48, fd_h=1e-5):
         fd_set = set(int(v) for v in rng.choice(nparams, size=min(fd_params, nparams),
                                                 replace=False))
         fd = finite_difference_gradient(s, recs, H, h=fd_h, params=fd_set)
+    # the same gradient on a complex<float> state (FP64 reductions), against
+    # the complex<double> one
+    recs32 = W.hea(n, 12, seed=7).gate_records(np.complex64, number_params=True)
+    with StateVector(n, np.complex64) as s32:
+        s32.set_stream(stream.cuda_stream)
+        for _ in range(2):
+            adjoint_gradient(s32, recs32, H)
+        torch.cuda.synchronize()
+        a.record(stream)
+        for _ in range(reps):
+            s32.set_basis(0)
+            e32, g32 = adjoint_gradient(s32, recs32, H)
+        b.record(stream)
+        torch.cuda.synchronize()
+        adj32_ms = a.elapsed_time(b) / reps
     err = float(max(abs(g[p] - ps[p]) for p in subset))
     fd_err = float(max(abs(g[p] - fd[p]) for p in fd_set))
     return {"workload": "hea24_12layers_c128_ising", "gates": len(recs), "params": nparams,
@@ -110,7 +125,10 @@ def adjoint_extra(torch, stream, ps_params, fd_params=48, fd_h=1e-5):
             "max_abs_grad_diff_vs_param_shift": err,
             "central_fd": {"h": fd_h, "params": len(fd_set), "seed": 24,
                            "max_abs_grad_diff_vs_adjoint": fd_err},
-            "max_abs_grad": float(np.max(np.abs(g)))}
+            "max_abs_grad": float(np.max(np.abs(g))),
+            "complex_float": {"adjoint_ms": adj32_ms,
+                              "max_abs_grad_diff_vs_c128": float(np.max(np.abs(g32 - g))),
+                              "energy_diff_vs_c128": abs(e32 - e)}}
 
 
 def plan_counts(n, code, recs, opts=None):
