@@ -96,6 +96,19 @@ def _rank_main(rank, world, port, out, n, use_gpu):
             y = s.download()
             if rank == 0:
                 res["zero"] = y
+            # a term with more X/Y factors than local qubits is refused on
+            # every rank alike (before any exchange for it)
+            from qclab_b200.observable import Observable
+            try:
+                s.expectation(Observable(n).add(1.0, "X" * n))
+                res["wide"] = "accepted"
+            except ValueError:
+                res["wide"] = "refused"
+            try:
+                ShardedStateVector(world.bit_length() + 1, np.complex128, **kw)
+                res["small"] = "accepted"
+            except ValueError:
+                res["small"] = "refused"
         if rank == 0:
             out.update({str(k): v for k, v in res.items()})
         dist.barrier()
@@ -134,6 +147,8 @@ def test_sharded_state_matches_whole_vector(world, n):
     z = np.zeros(1 << n, dtype=np.complex128)
     z[0] = 1
     assert np.max(np.abs(res["zero"] - oracle.apply(z, _circuit(n, 11)[:30], "N"))) <= 1e-13
+    assert res["wide"] == "refused"     # n X factors, n - g local qubits
+    assert res["small"] == "refused"    # fewer than 3 local qubits
 
 
 def test_sharded_rejects_bad_sizes():
